@@ -1,0 +1,312 @@
+// gf_kernels.cuh -- kernel templates shared by the plugin entry points (reference layout, in
+// place) and the batched engine (packed layout): parity pass, gauge quality with a deterministic
+// FP64 reduction, reprojection and random start.
+#pragma once
+
+#include "gf_field.cuh"
+
+namespace gfb {
+
+// ---- one parity pass ---------------------------------------------------------------------------
+// 4 lanes per site (lane = 8*mu + site-in-warp), 8 sites per warp.  Vh is a multiple of 8 for
+// even extents, so a warp is either fully inside the parity half or fully outside.
+// Fup holds the up links and every down link except, for COULOMB, the temporal down link, which
+// comes from the slice t-1 field Fdw at the same spatial site (CoulombKernelsSU3.hxx:226-234).
+template <typename R, int GAUGE, int ALGO, class F>
+__device__ __forceinline__ void parity_pass_warp(const F &Fup, const F &Fdw, const Geom &g, int64_t warp, int parity,
+                                                 const AlgoParams &p)
+{
+    const int lane = threadIdx.x & 31;
+    const int mu = lane >> 3;
+    const int64_t h = warp * 8 + (lane & 7);
+    int32_t c[4];
+    site_coords(g, h, parity, c);
+    const int64_t s = h + (parity ? g.Vh : 0);
+    const bool tdown = (GAUGE == COULOMB) && (mu == 0);
+    const int64_t sd = tdown ? s : neighbour_down(g, c, mu);
+    Link<R> up, dn;
+    load_link<R>(Fup, s, mu, up);
+    if (tdown)
+        load_link<R>(Fdw, sd, mu, dn);
+    else
+        load_link<R>(Fup, sd, mu, dn);
+    Rng<R> rng;
+    if (ALGO == ALG_SA || ALGO == ALG_SR || ALGO == ALG_RANDOM) rng.init(ref_rng_tid(h), p.seed, p.counter);
+    site_update<GAUGE, ALGO>(up, dn, mu, p, rng);
+    store_link<R>(Fup, s, mu, up);
+    if (tdown)
+        store_link<R>(Fdw, sd, mu, dn);
+    else
+        store_link<R>(Fup, sd, mu, dn);
+}
+
+template <typename R, int GAUGE, int ALGO, class F>
+__global__ void __launch_bounds__(128) k_parity_pass(F Fup, F Fdw, Geom g, int parity, AlgoParams p)
+{
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (warp * 8 >= g.Vh) return;
+    parity_pass_warp<R, GAUGE, ALGO>(Fup, Fdw, g, warp, parity, p);
+}
+
+// ---- gauge quality ---------------------------------------------------------------------------
+template <typename R, class F>
+__device__ __forceinline__ void load_link_f64(const F &f, int64_t s, int mu, Link<double> &L)
+{
+    R r[12];
+    f.load12(s, mu, r);
+    double d[12];
+#pragma unroll
+    for (int k = 0; k < 12; k++) d[k] = (double)r[k];
+    unpack12(L, d);
+    reconstruct(L);
+}
+
+// Per-site functional and theta, computed in FP64 from the stored rows:
+//  LANDAU/U1XU1 (LandauKernelsSU3.hxx:114-191, U1xU1KernelsSU3.hxx:114-191) and COULOMB
+//  (CoulombKernelsSU3.hxx:110-183, mu = 1..3): gff = sum_mu Re tr U_mu(x);
+//  theta = sum_ij |(A - A^dagger)_ij|^2, A = D - tr(D)/3, D = sum_mu U_mu(x) - U_mu(x-mu).
+//  MAG (MAGKernelsSU3.hxx:116-223): gff = sum_mu sum_j |U_mu(x)_jj|^2, theta = sum_k |X_k|.
+template <int GAUGE, typename R, class F>
+__device__ __forceinline__ void quality_site(const F &f, const Geom &g, int64_t s, double &gff, double &th)
+{
+    const int parity = s >= g.Vh;
+    int32_t c[4];
+    site_coords(g, s - (parity ? g.Vh : 0), parity, c);
+    gff = 0;
+    if (GAUGE == MAG) {
+        double X[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+#pragma unroll 1
+        for (int mu = 0; mu < 4; mu++) {
+            Link<double> u, d;
+            load_link_f64<R>(f, s, mu, u);
+            load_link_f64<R>(f, neighbour_down(g, c, mu), mu, d);
+            gff += abs2(u.e[0][0]) + abs2(u.e[1][1]) + abs2(u.e[2][2]);
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                const int i = k == 2 ? 1 : 0, j = k == 0 ? 1 : 2;  // (0,1), (0,2), (1,2)
+                const Cx<double> a = u.e[i][i], b = u.e[i][j], cc = u.e[j][i], e = u.e[j][j];
+                // up: m00 conj(m10) - m01 conj(m11)
+                X[k][0] += (a.x * cc.x + a.y * cc.y) - (b.x * e.x + b.y * e.y);
+                X[k][1] += (a.y * cc.x - a.x * cc.y) - (b.y * e.x - b.x * e.y);
+                // down, hermitian submatrix: conj(d_ii) d_ij - conj(d_ji) d_jj
+                const Cx<double> p = d.e[i][i], q = d.e[i][j], r = d.e[j][i], t = d.e[j][j];
+                X[k][0] += (p.x * q.x + p.y * q.y) - (r.x * t.x + r.y * t.y);
+                X[k][1] += (p.x * q.y - p.y * q.x) - (r.x * t.y - r.y * t.x);
+            }
+        }
+        th = sqrt(X[0][0] * X[0][0] + X[0][1] * X[0][1]) + sqrt(X[1][0] * X[1][0] + X[1][1] * X[1][1]) +
+             sqrt(X[2][0] * X[2][0] + X[2][1] * X[2][1]);
+    } else {
+        Cx<double> D[3][3];
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) D[i][j] = cx<double>(0, 0);
+        const int mu0 = GAUGE == COULOMB ? 1 : 0;
+#pragma unroll 1
+        for (int mu = mu0; mu < 4; mu++) {
+            Link<double> u;
+            load_link_f64<R>(f, s, mu, u);
+            gff += u.e[0][0].x + u.e[1][1].x + u.e[2][2].x;
+#pragma unroll
+            for (int i = 0; i < 3; i++)
+#pragma unroll
+                for (int j = 0; j < 3; j++) {
+                    D[i][j].x += u.e[i][j].x;
+                    D[i][j].y += u.e[i][j].y;
+                }
+            load_link_f64<R>(f, neighbour_down(g, c, mu), mu, u);
+#pragma unroll
+            for (int i = 0; i < 3; i++)
+#pragma unroll
+                for (int j = 0; j < 3; j++) {
+                    D[i][j].x -= u.e[i][j].x;
+                    D[i][j].y -= u.e[i][j].y;
+                }
+        }
+        const double trx = (D[0][0].x + D[1][1].x + D[2][2].x) / 3.0;
+        const double try_ = (D[0][0].y + D[1][1].y + D[2][2].y) / 3.0;
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            D[i][i].x -= trx;
+            D[i][i].y -= try_;
+        }
+        double acc = 0;
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                const double rx = D[i][j].x - D[j][i].x;  // (A - A^dagger)_ij = A_ij - conj(A_ji)
+                const double ry = D[i][j].y + D[j][i].y;
+                acc += rx * rx + ry * ry;
+            }
+        th = acc;
+    }
+}
+
+// Fixed-order block reduction (warp butterfly, then warps in order): deterministic for a fixed
+// launch shape.  Result valid in thread 0.
+template <int NT>
+__device__ __forceinline__ void block_reduce2(double &a, double &b, bool b_is_max)
+{
+    __shared__ double sa[NT / 32], sb[NT / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        const double ob = __shfl_xor_sync(0xffffffffu, b, o);
+        b = b_is_max ? fmax(b, ob) : b + ob;
+    }
+    const int w = threadIdx.x >> 5;
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) {
+        sa[w] = a;
+        sb[w] = b;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        a = sa[0];
+        b = sb[0];
+#pragma unroll
+        for (int k = 1; k < NT / 32; k++) {
+            a += sa[k];
+            b = b_is_max ? fmax(b, sb[k]) : b + sb[k];
+        }
+    }
+}
+
+struct QualityOut {
+    double *partials;    // 2 doubles per block
+    unsigned int *ticket; // zero before the launch; the last block resets it
+    double *result;      // [0] = functional, [1] = theta (normalised as the reference does)
+    double *gff_site;    // optional per-site arrays (generateGaugeQualityPerSite), may be null
+    double *theta_site;
+};
+
+// GaugeFixingStats::generateGaugeQuality (GaugeFixingStats.hxx:186-232) in one launch: per-site
+// values, per-block partial sums, and the last block to finish sums the partials in block
+// order and applies the normalisation gff*preG/V, theta*preA (/V for AVERAGE).
+template <int GAUGE, typename R, class F, int NT = 256>
+__global__ void __launch_bounds__(NT) k_quality(F f, Geom g, QualityOut o, int stop_max, double preG, double preA)
+{
+    const int64_t s = (int64_t)blockIdx.x * NT + threadIdx.x;
+    double gv = 0, tv = 0;
+    if (s < g.V) {
+        quality_site<GAUGE, R>(f, g, s, gv, tv);
+        if (o.gff_site) o.gff_site[s] = gv;
+        if (o.theta_site) o.theta_site[s] = tv;
+    }
+    block_reduce2<NT>(gv, tv, stop_max != 0);
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        o.partials[2 * blockIdx.x] = gv;
+        o.partials[2 * blockIdx.x + 1] = tv;
+        __threadfence();
+        last = atomicAdd(o.ticket, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double G = 0, T = 0;
+    for (unsigned int k = threadIdx.x; k < gridDim.x; k += NT) {
+        G += __ldcg(&o.partials[2 * k]);
+        const double t = __ldcg(&o.partials[2 * k + 1]);
+        T = stop_max ? fmax(T, t) : T + t;
+    }
+    block_reduce2<NT>(G, T, stop_max != 0);
+    if (threadIdx.x == 0) {
+        double gn = G * preG / (double)g.V;
+        double tn = T * preA;
+        if (!stop_max) tn = tn / (double)g.V;
+        o.result[0] = gn;
+        o.result[1] = tn;
+        *o.ticket = 0;
+    }
+}
+
+// ---- reprojection (SU3::projectSU3, lattice/SU3.hxx:536-583) in FP64 ---------------------------
+__device__ __forceinline__ void project_rows(Link<double> &L)
+{
+    double nu = 0;
+#pragma unroll
+    for (int i = 0; i < 3; i++) nu += abs2(L.e[0][i]);
+    nu = 1.0 / sqrt(nu);
+#pragma unroll
+    for (int i = 0; i < 3; i++) L.e[0][i] = cx<double>(L.e[0][i].x * nu, L.e[0][i].y * nu);
+    Cx<double> sp = cx<double>(0, 0);  // sum_i row1_i conj(row0_i)
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        sp.x += L.e[1][i].x * L.e[0][i].x + L.e[1][i].y * L.e[0][i].y;
+        sp.y += L.e[1][i].y * L.e[0][i].x - L.e[1][i].x * L.e[0][i].y;
+    }
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        const Cx<double> t = cmul(L.e[0][i], sp);
+        L.e[1][i].x -= t.x;
+        L.e[1][i].y -= t.y;
+    }
+    double nv = 0;
+#pragma unroll
+    for (int i = 0; i < 3; i++) nv += abs2(L.e[1][i]);
+    nv = 1.0 / sqrt(nv);
+#pragma unroll
+    for (int i = 0; i < 3; i++) L.e[1][i] = cx<double>(L.e[1][i].x * nv, L.e[1][i].y * nv);
+    reconstruct(L);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_project_ref(RefField<R> f)
+{
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= 4 * f.V) return;
+    const int mu = (int)(idx / f.V);
+    const int64_t s = idx - mu * f.V;
+    Link<double> L;
+    load_link_f64<R>(f, s, mu, L);
+    project_rows(L);
+    Link<R> o;
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) o.e[i][j] = cx<R>((R)L.e[i][j].x, (R)L.e[i][j].y);
+    f.store18(s, mu, o);
+}
+
+// ---- random start (COMKSU3::setHot, CommonKernelsSU3.hxx:92-130) -------------------------------
+template <int I, int J, typename R>
+__device__ __forceinline__ void hot_subgroup(Link<R> &M, Rng<R> &rng)
+{
+    R q[4];
+    q[0] = (R)(rng.rand() * 2.0 - 1.0);
+    q[1] = (R)(rng.rand() * 2.0 - 1.0);
+    q[2] = (R)(rng.rand() * 2.0 - 1.0);
+    q[3] = (R)(rng.rand() * 2.0 - 1.0);
+    const R det = rsq(q[0] * q[0] + q[3] * q[3] + q[2] * q[2] + q[1] * q[1]);  // Quaternion::projectSU2
+    q[0] *= det;
+    q[1] *= det;
+    q[2] *= det;
+    q[3] *= det;
+    right_mult<I, J>(M, q);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_set_hot_ref(RefField<R> f, uint32_t seed, uint32_t counter)
+{
+    const int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= f.V) return;
+    Rng<R> rng;
+    rng.init((uint32_t)s, seed, counter);
+#pragma unroll 1
+    for (int mu = 0; mu < 4; mu++) {
+        Link<R> M;
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) M.e[i][j] = cx<R>(i == j ? (R)1 : (R)0, (R)0);
+        hot_subgroup<0, 1>(M, rng);
+        hot_subgroup<0, 2>(M, rng);
+        hot_subgroup<1, 2>(M, rng);
+        f.store18(s, mu, M);
+    }
+}
+
+}  // namespace gfb

@@ -1,0 +1,154 @@
+"""ctypes access to the CPU oracle (oracle/liborc.so) and to the reference-pin
+libraries (oracle/_ref/libref_pin_{f64,f32}.so) for the tests.
+
+Test infrastructure only: the oracle is the checker, never the thing measured.
+"""
+from __future__ import annotations
+
+import ctypes
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[1]
+ORACLE_DIR = ROOT / "oracle"
+ORACLE_SO = ORACLE_DIR / "liborc.so"
+REF_DIR = ORACLE_DIR / "_ref"
+
+LANDAU, COULOMB, MAG, U1XU1 = 0, 1, 2, 3
+OR, MICRO, SA, SR, RANDOM = 0, 1, 2, 3, 4
+GAUGES = {"landau": LANDAU, "coulomb": COULOMB, "mag": MAG, "u1xu1": U1XU1}
+ALGOS = {"or": OR, "micro": MICRO, "sa": SA, "sr": SR, "random": RANDOM}
+
+_P = ctypes.c_void_p
+_u32 = ctypes.c_uint32
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(_P)
+
+
+def _size(size):
+    return np.ascontiguousarray(size, dtype=np.int32)
+
+
+_ORC = None
+
+
+def oracle() -> ctypes.CDLL:
+    """Load (building with make if needed) the C oracle."""
+    global _ORC
+    if _ORC is None:
+        if not ORACLE_SO.exists():
+            subprocess.run(["make", "-C", str(ORACLE_DIR), "liborc.so"], check=True, capture_output=True)
+        _ORC = ctypes.CDLL(str(ORACLE_SO))
+    return _ORC
+
+
+def ref_pin(prec: str):
+    """The reference's own site-update code compiled for the host, or None if not built."""
+    p = REF_DIR / f"libref_pin_{prec}.so"
+    return ctypes.CDLL(str(p)) if p.exists() else None
+
+
+def volume(size) -> int:
+    return int(np.prod(size))
+
+
+def field_zeros(size, dtype=np.float64):
+    return np.zeros(volume(size) * 72, dtype=dtype)
+
+
+def sfx(a) -> str:
+    return "f64" if a.dtype == np.float64 else "f32"
+
+
+def set_hot(size, seed, counter, dtype=np.float64, nthreads=8):
+    U = field_zeros(size, dtype)
+    getattr(oracle(), "orc_set_hot_" + sfx(U))(_ptr(U), _ptr(_size(size)), _u32(seed), _u32(counter), nthreads)
+    return U
+
+
+def step(U, size, gauge, algo, parity, param=0.0, seed=0, counter=0, Udw=None, nthreads=8):
+    """One parity pass in place (Udw: slice t-1 for Coulomb)."""
+    getattr(oracle(), "orc_step_" + sfx(U))(_ptr(U), _ptr(Udw), _ptr(_size(size)), gauge, algo, parity,
+                                            ctypes.c_float(param), _u32(seed), _u32(counter), nthreads)
+
+
+def quality(U, size, gauge, stop_max=0, per_site=False, nthreads=8):
+    V = volume(size)
+    g, a = ctypes.c_double(), ctypes.c_double()
+    gs = np.zeros(V) if per_site else None
+    as_ = np.zeros(V) if per_site else None
+    getattr(oracle(), "orc_quality_" + sfx(U))(_ptr(U), _ptr(_size(size)), gauge, stop_max, ctypes.byref(g),
+                                               ctypes.byref(a), _ptr(gs), _ptr(as_), nthreads)
+    if per_site:
+        return g.value, a.value, gs, as_
+    return g.value, a.value
+
+
+def project(U, size, nthreads=8):
+    getattr(oracle(), "orc_project_" + sfx(U))(_ptr(U), _ptr(_size(size)), nthreads)
+
+
+class Schedule(ctypes.Structure):
+    _fields_ = [("random_trafo", ctypes.c_int), ("sa_steps", ctypes.c_int), ("sa_min", ctypes.c_float),
+                ("sa_max", ctypes.c_float), ("micro_updates", ctypes.c_int), ("or_max_iter", ctypes.c_int),
+                ("or_parameter", ctypes.c_float), ("precision", ctypes.c_float),
+                ("check_precision", ctypes.c_int), ("reproject", ctypes.c_int), ("seed", ctypes.c_uint32)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [("gff", ctypes.c_double), ("theta", ctypes.c_double), ("or_iterations", ctypes.c_int)]
+
+
+def fix(U, size, gauge, sched: Schedule, counter=0, nthreads=8):
+    c = _u32(counter)
+    r = Result()
+    getattr(oracle(), "orc_fix_" + sfx(U))(_ptr(U), _ptr(_size(size)), gauge, ctypes.byref(sched), ctypes.byref(c),
+                                           ctypes.byref(r), nthreads)
+    return r, c.value
+
+
+# ---- the reference's own code on the host (oracle/_ref) ----------------------------------------
+def ref_step(U, size, gauge, algo, parity, param=0.0, seed=0, counter=0, Udw=None):
+    lib = ref_pin(sfx(U))
+    rc = getattr(lib, "ref_step_" + sfx(U))(_ptr(U), _ptr(Udw), _ptr(_size(size)), gauge, algo, parity,
+                                             ctypes.c_float(param), _u32(seed), _u32(counter))
+    assert rc == 0
+
+
+def ref_quality_sites(U, size, gauge):
+    lib = ref_pin(sfx(U))
+    V = volume(size)
+    g = np.zeros(V)
+    a = np.zeros(V)
+    getattr(lib, "ref_quality_sites_" + sfx(U))(_ptr(U), _ptr(_size(size)), gauge, _ptr(g), _ptr(a))
+    return g, a
+
+
+def ref_project(U, size):
+    getattr(ref_pin(sfx(U)), "ref_project_" + sfx(U))(_ptr(U), _ptr(_size(size)))
+
+
+def ref_set_hot(size, seed, counter, dtype=np.float64):
+    U = field_zeros(size, dtype)
+    getattr(ref_pin(sfx(U)), "ref_set_hot_" + sfx(U))(_ptr(U), _ptr(_size(size)), _u32(seed), _u32(counter))
+    return U
+
+
+# ---- layout helpers (reference GpuPattern) -----------------------------------------------------
+def links(U, size):
+    """GpuPattern array -> complex array [mu][V][3][3]."""
+    V = volume(size)
+    a = U.reshape(4, 3, 3, 2, V).astype(np.float64)
+    return np.transpose(a[..., 0, :] + 1j * a[..., 1, :], (0, 3, 1, 2))
+
+
+def rows01_maxdiff(A, B, size):
+    """max |A - B| over the stored rows 0,1 (what the sweep reads and writes)."""
+    V = volume(size)
+    a = A.reshape(4, 3, 3, 2, V)[:, :2].astype(np.float64)
+    b = B.reshape(4, 3, 3, 2, V)[:, :2].astype(np.float64)
+    return float(np.abs(a - b).max())

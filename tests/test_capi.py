@@ -1,0 +1,65 @@
+"""The C-ABI library loads and exports every entry point include/*.h declares;
+argument validation works without touching the GPU (no compute calls here)."""
+import ctypes
+import re
+import subprocess
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def _declared_functions():
+    names = []
+    for h in sorted((ROOT / "include").glob("*.h")):
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        names += re.findall(r"^[A-Za-z_][\w \*]*?\b(gf\w+)\s*\(", text, flags=re.M)
+    return sorted(set(names))
+
+
+def test_header_declares_entry_points():
+    names = _declared_functions()
+    for must in ("gf_or_step", "gf_sa_step", "gf_stats_generate", "gf_project_su3", "gf_last_error_string"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol():
+    from su3_ma_gauge_gpu_b200 import _lib
+
+    L = _lib.lib()
+    missing = [n for n in _declared_functions() if not hasattr(L, n)]
+    assert not missing, f"declared in include/ but not exported: {missing}"
+    # the ctypes signature table covers the same set
+    assert set(_lib.SIGNATURES) >= set(_declared_functions())
+
+
+def test_library_is_built_for_sm100a():
+    from su3_ma_gauge_gpu_b200 import _lib
+
+    out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", str(_lib.LIB_PATH)],
+                         capture_output=True, text=True)
+    if out.returncode != 0:
+        pytest.skip("cuobjdump unavailable")
+    assert "sm_100a" in out.stdout
+
+
+def test_validation_without_gpu():
+    from su3_ma_gauge_gpu_b200 import _lib
+
+    L = _lib.lib()
+    assert L.gf_version().startswith(b"su3_ma_gauge_gpu_b200")
+    bogus = ctypes.c_void_p(0x1000)  # never dereferenced: validation fails first
+    s = _lib.size_arg((4, 4, 4, 3))
+    assert L.gf_or_step(0, 1, bogus, None, s, 0, ctypes.c_float(1.7), None) == _lib.GF_ERR_INVALID
+    assert b"even" in L.gf_last_error_string()
+    s = _lib.size_arg((4, 4, 4, 4))
+    assert L.gf_or_step(7, 1, bogus, None, s, 0, ctypes.c_float(1.7), None) == _lib.GF_ERR_INVALID
+    assert L.gf_or_step(0, 5, bogus, None, s, 0, ctypes.c_float(1.7), None) == _lib.GF_ERR_INVALID
+    assert L.gf_or_step(0, 1, None, None, s, 0, ctypes.c_float(1.7), None) == _lib.GF_ERR_INVALID
+    assert L.gf_or_step(1, 1, bogus, bogus, s, 0, ctypes.c_float(1.7), None) == _lib.GF_ERR_INVALID  # slice
+    assert L.gf_or_step(1, 1, bogus, None, _lib.size_arg((1, 4, 4, 4)), 0, ctypes.c_float(1.7), None) \
+        == _lib.GF_ERR_INVALID  # Coulomb without UtDw
+    assert L.gf_quality_prefactor_gff(0) == pytest.approx(1 / 12)
+    assert L.gf_quality_prefactor_gff(1) == pytest.approx(1 / 9)
+    assert L.gf_quality_prefactor_a(2) == pytest.approx(1 / 3)
