@@ -1,0 +1,374 @@
+#!/usr/bin/env python
+"""Benchmark: time to gauge-fix a 32^4 Landau configuration to theta < 1e-12.
+
+Workload (one "step"): the 32^4 lattice built from U = exp(i*0.3*H) (H traceless
+Hermitian, N(0,1) entries) under a seeded Haar gauge transformation, gauge-fixed
+with overrelaxation (omega = 1.7) in mixed precision -- FP32 12-real storage until
+theta < 1e-9, then FP64 polish sweeps to theta < 1e-12 -- through the library's
+context API: import of the reference-layout (GpuPattern, FP64) field, gf_fix,
+export of the reunitarised field.  The same input is also fixed in plain FP64 to
+report the mixed/FP64 time-to-theta ratio and the functional error.
+
+Metric: site updates per second over the whole job (sum over ranks of
+V x OR sweeps done / max-over-ranks time).  ``value`` has the input resident in
+HBM; ``e2e`` runs the same call with pinned host buffers (H2D of rows 0,1 of the
+input and D2H of the full output inside the timed region).
+
+Multi-GPU: one process per GPU, each fixing its own configuration (seed + rank);
+gauge copies are independent, so there is no data-path collective ("weak").
+
+``--impl reference`` times the reference's path on the host cores instead: the
+reference has no CPU implementation, so this is the C restatement of its device
+code (oracle/, built with OpenMP over the sites of one parity), each step one FP64
+OR sweep of the same 32^4 field.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Gsite-updates/s & HBM GB/s; time-to-theta<1e-12 mixed/batched vs plain FP64"
+UNIT = "Gsite-updates/s"
+SIZE = (32, 32, 32, 32)
+EPS = 0.3
+BYTES_PER_SITE_UPDATE = {"fp32": 768, "fp64": 1536}  # 8 links x 12 reals x (read + write)
+
+
+def env_rank():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")),
+            int(os.environ.get("WORLD_SIZE", "1")))
+
+
+def measured_peak_hbm():
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str | None):
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+        if gpu_id:
+            cmd += ["-i", gpu_id]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait(timeout=10)
+        self.file.flush()
+        rows = [r.split(", ") for r in Path(self.file.name).read_text().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.file.name)
+        sm, smax, power, reasons = [], [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax.append(float(r[2]))
+                power.append(float(r[3]))
+            except ValueError:
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.strip() == "Active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        pmax = max(power)
+        loaded = [s for s, p in zip(sm, power) if p >= 0.5 * pmax] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm), "power_w_max": pmax}
+
+
+def cpu_oracle():
+    sys.path.insert(0, str(ROOT / "tests"))
+    import _oracle  # the oracle is loaded only for the CPU-baseline leg and the reference arm
+
+    return _oracle
+
+
+def cpu_or_rate(U, size, budget_s: float):
+    """FP64 OR sweeps of the C restatement on all host cores for about budget_s seconds."""
+    O = cpu_oracle()
+    n_thr = os.cpu_count() or 1
+    V = O.volume(size)
+    W = U.copy()
+    t0 = time.perf_counter()
+    for parity in (0, 1):
+        O.step(W, size, O.LANDAU, O.OR, parity, 1.7, nthreads=n_thr)
+    one = time.perf_counter() - t0
+    n = max(1, int(budget_s / max(one, 1e-6)) - 1)
+    t0 = time.perf_counter()
+    for _ in range(n):
+        for parity in (0, 1):
+            O.step(W, size, O.LANDAU, O.OR, parity, 1.7, nthreads=n_thr)
+    t = time.perf_counter() - t0
+    return {"value": V * n / t / 1e9, "unit": UNIT, "cores": n_thr, "kind": "port",
+            "sample": f"{n} FP64 OR sweeps (omega=1.7) of the 32^4 input on {n_thr} host threads"}
+
+
+def run_reference(args):
+    rank, _, world = env_rank()
+    if rank != 0:
+        return
+    from su3_ma_gauge_gpu_b200 import synthetic as S
+
+    O = cpu_oracle()
+    U, _ = S.smooth_config(SIZE, EPS, 1234)
+    V = O.volume(SIZE)
+    n_thr = os.cpu_count() or 1
+    W = U.copy()
+
+    def step():
+        for parity in (0, 1):
+            O.step(W, SIZE, O.LANDAU, O.OR, parity, 1.7, nthreads=n_thr)
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    t = (time.perf_counter() - t0) / args.steps
+    val = V / t / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "Landau OR sweep of a 32^4 SU(3) lattice (eps=0.3 smooth field under a Haar "
+                               "gauge transform), FP64; one step = one sweep (both parities)",
+                   "lattice": list(SIZE)},
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": n_thr, "kind": "port",
+                         "sample": "C restatement of the reference device code (the reference has no CPU path), "
+                                   f"OpenMP over sites, {n_thr} threads, one FP64 OR sweep per step"},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--check", type=int, default=20, help="sweeps between quality checks")
+    ap.add_argument("--cpu-budget", type=float, default=10.0)
+    ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison run")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import numpy as np
+    import torch
+
+    rank, local_rank, world = env_rank()
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from su3_ma_gauge_gpu_b200 import synthetic as S
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer, Schedule
+
+    V = int(np.prod(SIZE))
+    U_host, f0 = S.smooth_config(SIZE, EPS, 1234 + rank, device="cuda")
+    U_pin = torch.from_numpy(U_host).pin_memory()
+    U_pin_np = U_pin.numpy()
+    out_pin = torch.empty_like(U_pin).pin_memory()
+    out_pin_np = out_pin.numpy()
+    dU_in = U_pin.cuda()
+    dU_out = torch.empty_like(dU_in)
+    stream = torch.cuda.Stream()
+    sched = Schedule(or_max_iter=20000, precision=1e-12, switch_theta=1e-9, check_precision=args.check,
+                     reproject=100, micro_updates=0)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    def timed(gf, step_fn, steps, warmup):
+        reps = None
+        for _ in range(warmup):
+            reps = step_fn(gf)
+        barrier()
+        torch.cuda.synchronize()
+        l0 = gf.kernel_launches()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            reps = step_fn(gf)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms = e0.elapsed_time(e1) / steps
+        return ms, reps, (gf.kernel_launches() - l0) / steps
+
+    def step_resident(gf):
+        gf.load(0, dU_in)
+        r = gf.fix(sched)[0]
+        gf.store(0, dU_out)
+        return r
+
+    def step_host(gf):
+        gf.load(0, U_pin_np)
+        r = gf.fix(sched)[0]
+        gf.store(0, out_pin_np)
+        return r
+
+    gpu_id = None
+    try:
+        gpu_id = "GPU-" + str(torch.cuda.get_device_properties(local_rank).uuid)
+    except Exception:
+        pass
+
+    gf = GaugeFixer([SIZE], mixed=True, stream=stream)
+    clocks = ClockSampler(gpu_id)
+    ms, rep, launches = timed(gf, step_resident, args.steps, args.warmup)
+    clk = clocks.stop()
+    ms_e2e, rep_e2e, _ = timed(gf, step_host, max(1, args.steps - 1), 1)
+
+    # dominant kernels: OR parity passes timed alone on the same stream (CUDA events), per launch
+    def pass_ms(nsweeps=20):
+        gf.load(0, dU_in)
+        gf.sweeps("or", 2, 1.7)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        gf.sweeps("or", nsweeps, 1.7)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / (2 * nsweeps)
+
+    t32 = pass_ms()
+    gf.close()
+
+    res64 = None
+    ms64 = None
+    if not args.no_fp64:
+        gf64 = GaugeFixer([SIZE], mixed=False, stream=stream)
+        ms64, res64, _ = timed(gf64, step_resident, 1, 1)
+        gf64.load(0, dU_in)
+        gf64.sweeps("or", 2, 1.7)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        gf64.sweeps("or", 10, 1.7)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t64 = e0.elapsed_time(e1) / 20
+        gf64.close()
+    else:
+        t64 = None
+
+    sweeps = rep.or_sweeps
+    site_updates = V * sweeps
+    ms_max = max_over_ranks(ms)
+    ms_e2e_max = max_over_ranks(ms_e2e)
+    total_updates = sum_over_ranks(float(site_updates))
+    value = total_updates / (ms_max * 1e-3) / 1e9
+    e2e = sum_over_ranks(float(V * rep_e2e.or_sweeps)) / (ms_e2e_max * 1e-3) / 1e9
+
+    peak, peak_kind = measured_peak_hbm()
+    Vh = V // 2
+    n64 = rep.or_sweeps_fp64
+    n32 = sweeps - n64
+    kern = {"fp32": {"ms_per_launch": t32, "gbs": Vh * BYTES_PER_SITE_UPDATE["fp32"] / (t32 * 1e-3) / 1e9,
+                     "launches_per_step": 2 * n32}}
+    if t64 is not None:
+        kern["fp64"] = {"ms_per_launch": t64, "gbs": Vh * BYTES_PER_SITE_UPDATE["fp64"] / (t64 * 1e-3) / 1e9,
+                        "launches_per_step": 2 * n64}
+    dom = max(kern, key=lambda k: kern[k]["ms_per_launch"] * kern[k]["launches_per_step"])
+    traffic = None
+    tfile = ROOT / "profiles" / "or_pass_traffic.json"
+    if tfile.exists():
+        try:
+            traffic = json.loads(tfile.read_text()).get(dom)
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "achieved": kern[dom]["gbs"], "peak": peak, "unit": "GB/s",
+                "frac": kern[dom]["gbs"] / peak, "traffic": traffic,
+                "kernel": f"k_batched_pass<{'float' if dom == 'fp32' else 'double'}, LANDAU, OR> (one parity pass)",
+                "algorithmic_bytes_per_launch": Vh * BYTES_PER_SITE_UPDATE[dom], "peak_kind": peak_kind,
+                "per_precision": kern}
+
+    cpu = None
+    if rank == 0 and world == 1:
+        cpu = cpu_or_rate(U_host, SIZE, args.cpu_budget)
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": "Landau gauge fix of a 32^4 SU(3) lattice to theta<1e-12: U=exp(i*0.3*H) under a "
+                               "seeded Haar gauge transform, OR omega=1.7, FP32 12-real storage to theta<1e-9 then "
+                               "FP64 polish; one step = import + gf_fix + export",
+                   "lattice": list(SIZE), "instances_per_gpu": 1, "check_every": args.check,
+                   "l2": "inputs larger than L2 (FP32 field 201 MB, FP64 403 MB > 126 MB)"},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": V * 4 * 12 * 8, "d2h_bytes_per_step": V * 72 * 8,
+                "ms_per_step": ms_e2e_max},
+        "gpu_launches": int(round(launches)),
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "clocks": clk,
+        "time_to_theta": {
+            "mixed_ms": ms_max, "fp64_ms": ms64,
+            "fp64_over_mixed": (ms64 / ms_max) if ms64 else None,
+            "mixed": {"or_sweeps": sweeps, "fp64_sweeps": n64, "theta": rep.theta, "F": rep.gff},
+            "fp64": ({"or_sweeps": res64.or_sweeps, "theta": res64.theta, "F": res64.gff} if res64 else None),
+            "F_rel_err_vs_fp64": (abs(rep.gff - res64.gff) / abs(res64.gff)) if res64 else None,
+            "F_pre_transform": f0,
+            "F_rel_vs_pre_transform": (rep.gff - f0) / f0,
+        },
+    }
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -101,6 +101,76 @@ int gf_stats_create(int gauge, int real, const int32_t size[4], int stopping, gf
 int gf_stats_generate(gf_stats *st, const void *U, void *stream, double *gff, double *theta);
 int gf_stats_destroy(gf_stats *st);
 
+/* ---- context level: batched, mixed-precision gauge fixing --------------------------------
+ * A context holds one or more lattices ("instances": gauge copies, lattices of uneven extents)
+ * in this library's packed 12-real layout.  Every parity pass is one launch over all instances;
+ * convergence is decided per instance on the device, and converged instances drop out.
+ * mixed = 1: instances sweep in FP32 until theta < switch_theta, then move (reunitarised in
+ * FP64) to FP64 storage for the polish to theta < precision; mixed = 0: FP64 throughout.
+ * The gauge functional and theta always accumulate in FP64.
+ * This replaces the per-copy loop of the reference drivers
+ * (apps/LandauGaugeFixingSU3_4D.cu:185-283, apps/MAGaugeFixingSU3_4D.cu:197-333), which fix
+ * one configuration of compile-time extents at a time.  GF_COULOMB is not accepted here. */
+typedef struct gf_ctx gf_ctx;
+
+typedef struct gf_ctx_params {
+    int gauge;             /* GF_LANDAU, GF_MAG or GF_U1XU1 */
+    int ninstances;        /* >= 1 */
+    const int32_t *sizes;  /* 4 * ninstances extents {Nt, Nx, Ny, Nz}, all even */
+    int mixed;             /* 1: FP32 bulk + FP64 polish, 0: FP64 only */
+    void *stream;          /* cudaStream_t to run on, or NULL for a stream of the context's own */
+} gf_ctx_params;
+
+/* the knobs of the reference's ProgramOptions (apps/program_options/ProgramOptions.hxx:223-266)
+ * that drive the per-copy loop, plus the mixed-precision switch */
+typedef struct gf_schedule {
+    int random_trafo;      /* randomtrafo: random gauge transformation first */
+    uint32_t seed;         /* seed (Philox key word 1; instance i uses seed + i) */
+    uint32_t rng_counter;  /* first Philox launch counter (PhiloxWrapper::getNextCounter) */
+    int sa_steps;          /* sasteps */
+    float sa_min, sa_max;  /* samin, samax */
+    int sa_geometric;      /* 0: linear temperature steps (reference), 1: geometric */
+    int micro_updates;     /* microupdates after each SA sweep */
+    int or_max_iter;       /* ormaxiter: OR sweep budget (FP32 + FP64) */
+    float or_parameter;    /* orparameter (omega) */
+    double precision;      /* stop when theta < precision */
+    double switch_theta;   /* mixed contexts: FP32 -> FP64 when theta < switch_theta */
+    int check_precision;   /* checkprecision: sweeps between checks */
+    int reproject;         /* reproject: sweeps between reunitarisations */
+    int use_graphs;        /* 1: replay check chunks from CUDA graphs */
+} gf_schedule;
+
+typedef struct gf_report {
+    double gff, theta;     /* FP64 functional and theta at the last check */
+    int or_sweeps;         /* OR sweeps done (FP32 + FP64) */
+    int or_sweeps_fp64;    /* of which in FP64 */
+    int sa_sweeps;         /* SA sweeps done */
+    int converged;         /* theta < precision */
+    int chunks;            /* check chunks launched */
+} gf_report;
+
+int gf_create(const gf_ctx_params *params, gf_ctx **out);
+int gf_destroy(gf_ctx *ctx);
+/* Load instance `instance` from a GpuPattern array (float or double; device memory, or host
+ * memory with on_host = 1, in which case only rows 0,1 are copied).  Resets its state. */
+int gf_import(gf_ctx *ctx, int instance, int real, const void *U, int on_host);
+/* Write instance `instance` back as a GpuPattern array, reunitarised in FP64 with row 2
+ * rebuilt (the reference's closing projectSU3, apps/LandauGaugeFixingSU3_4D.cu:271). */
+int gf_export(gf_ctx *ctx, int instance, int real, void *U, int on_host);
+/* nsweeps full sweeps (both parities) of one algorithm (0 OR, 1 micro, 2 SA, 3 SR, 4 random
+ * trafo) on every instance still sweeping; Philox counters rng_counter, rng_counter+1, ... */
+int gf_sweeps(gf_ctx *ctx, int algo, int nsweeps, float param, int seed, int rng_counter);
+/* FP64 functional and theta of every instance (arrays of ninstances doubles). */
+int gf_quality_all(gf_ctx *ctx, double *gff, double *theta);
+/* Reunitarise every instance in its current storage (FP64 arithmetic). */
+int gf_reunitarize(gf_ctx *ctx);
+/* Move every FP32 instance of a mixed context to FP64 storage (reunitarised in FP64). */
+int gf_set_storage(gf_ctx *ctx, int real);
+/* The whole per-copy schedule for all instances; reports has ninstances entries (or NULL). */
+int gf_fix(gf_ctx *ctx, const gf_schedule *schedule, gf_report *reports);
+/* Number of kernels this context has launched so far (each node of a replayed graph counts). */
+int gf_kernel_launches(gf_ctx *ctx, long long *count);
+
 #ifdef __cplusplus
 }
 #endif

@@ -48,6 +48,46 @@ SIGNATURES = {
     "gf_stats_destroy": (_c_int, [_vp]),
 }
 
+
+
+class CtxParams(ctypes.Structure):
+    """gf_ctx_params of include/gfix.h."""
+
+    _fields_ = [("gauge", ctypes.c_int), ("ninstances", ctypes.c_int), ("sizes", _i32p), ("mixed", ctypes.c_int),
+                ("stream", ctypes.c_void_p)]
+
+
+class Schedule(ctypes.Structure):
+    """gf_schedule of include/gfix.h (the reference's ProgramOptions knobs)."""
+
+    _fields_ = [("random_trafo", ctypes.c_int), ("seed", ctypes.c_uint32), ("rng_counter", ctypes.c_uint32),
+                ("sa_steps", ctypes.c_int), ("sa_min", ctypes.c_float), ("sa_max", ctypes.c_float),
+                ("sa_geometric", ctypes.c_int), ("micro_updates", ctypes.c_int), ("or_max_iter", ctypes.c_int),
+                ("or_parameter", ctypes.c_float), ("precision", ctypes.c_double), ("switch_theta", ctypes.c_double),
+                ("check_precision", ctypes.c_int), ("reproject", ctypes.c_int), ("use_graphs", ctypes.c_int)]
+
+
+class Report(ctypes.Structure):
+    """gf_report of include/gfix.h."""
+
+    _fields_ = [("gff", ctypes.c_double), ("theta", ctypes.c_double), ("or_sweeps", ctypes.c_int),
+                ("or_sweeps_fp64", ctypes.c_int), ("sa_sweeps", ctypes.c_int), ("converged", ctypes.c_int),
+                ("chunks", ctypes.c_int)]
+
+
+SIGNATURES.update({
+    "gf_create": (_c_int, [ctypes.POINTER(CtxParams), ctypes.POINTER(_vp)]),
+    "gf_destroy": (_c_int, [_vp]),
+    "gf_import": (_c_int, [_vp, _c_int, _c_int, _vp, _c_int]),
+    "gf_export": (_c_int, [_vp, _c_int, _c_int, _vp, _c_int]),
+    "gf_sweeps": (_c_int, [_vp, _c_int, _c_int, _c_float, _c_int, _c_int]),
+    "gf_quality_all": (_c_int, [_vp, _dp, _dp]),
+    "gf_reunitarize": (_c_int, [_vp]),
+    "gf_set_storage": (_c_int, [_vp, _c_int]),
+    "gf_fix": (_c_int, [_vp, ctypes.POINTER(Schedule), ctypes.POINTER(Report)]),
+    "gf_kernel_launches": (_c_int, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
+})
+
 _LIB = None
 
 

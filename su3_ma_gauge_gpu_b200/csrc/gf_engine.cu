@@ -1,0 +1,659 @@
+// gf_engine.cu -- the context-level C ABI: batched, mixed-precision gauge fixing.
+//
+// A context holds one or more lattices ("instances": gauge copies, uneven extents), each in the
+// packed 12-real layout, FP32 and/or FP64.  gf_fix runs the reference driver's schedule
+// (apps/LandauGaugeFixingSU3_4D.cu:185-271: random trafo, SA + micro, OR with reproject and
+// checks, closing reprojection) for all instances at once:
+//  - every parity pass is ONE launch over all instances still sweeping in that precision;
+//  - a check (quality + state transition) every check_precision sweeps decides on the device
+//    whether an instance switches FP32 -> FP64 (theta < switch_theta) or is done
+//    (theta < precision, or out of sweeps); converged instances drop out of later launches;
+//  - the OR loop is captured as a CUDA graph of one check chunk and replayed; the host only
+//    reads the per-instance states (pinned memory) one chunk behind.
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "gf_engine.cuh"
+#include "gf_host.hpp"
+
+using namespace gfb;
+
+struct gf_ctx {
+    int gauge = 0, ninst = 0, mixed = 0, device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::vector<InstDesc> h_inst;
+    InstDesc *d_inst = nullptr;
+    int64_t total_warps = 0, total_links = 0, total_qblocks = 0, max_V = 0;
+    float4 *f32 = nullptr;
+    double2 *f64 = nullptr;
+    int *d_state = nullptr, *d_sweeps = nullptr, *d_sweeps64 = nullptr, *d_storage = nullptr;
+    double *d_quality = nullptr, *d_partials = nullptr;
+    unsigned int *d_tickets = nullptr;
+    int *h_state = nullptr;       // pinned (state, then storage: 2 * ninst)
+    double *h_quality = nullptr;  // pinned
+    int *h_sweeps = nullptr;      // pinned (2 * ninst: sweeps, sweeps64)
+    void *staging = nullptr;
+    size_t staging_bytes = 0;
+    cudaEvent_t ev_chunk[2] = {nullptr, nullptr};
+    mutable long long launches = 0;  // kernels this context has launched (graph nodes per replay)
+
+    EngineDev dev() const
+    {
+        EngineDev e;
+        e.inst = d_inst;
+        e.ninst = ninst;
+        e.state = d_state;
+        e.sweeps = d_sweeps;
+        e.sweeps64 = d_sweeps64;
+        e.storage = d_storage;
+        e.quality = d_quality;
+        e.partials = d_partials;
+        e.tickets = d_tickets;
+        return e;
+    }
+};
+
+namespace {
+
+constexpr int QNT = 256;
+
+unsigned grid_for(int64_t threads, int block) { return (unsigned)((threads + block - 1) / block); }
+
+// ---- batched kernel dispatch -------------------------------------------------------------------
+struct PassArgs {
+    const gf_ctx *c;
+    int parity;
+    AlgoParams p;
+    int want_state;
+};
+
+template <int GAUGE, int ALGO>
+struct BatchedPass {
+    static int run(const PassArgs &a)
+    {
+        const unsigned blocks = grid_for(a.c->total_warps * 32, 128);
+        if (a.want_state == ST_FP32)
+            k_batched_pass<float, GAUGE, ALGO><<<blocks, 128, 0, a.c->stream>>>(a.c->dev(), a.c->total_warps,
+                                                                             a.parity, a.p, a.want_state);
+        else
+            k_batched_pass<double, GAUGE, ALGO><<<blocks, 128, 0, a.c->stream>>>(a.c->dev(), a.c->total_warps,
+                                                                              a.parity, a.p, a.want_state);
+        return launch_status("batched parity pass");
+    }
+};
+
+int launch_sweep(const gf_ctx *c, int algo, int want_state, float param, uint32_t seed, uint32_t counter_even,
+                 uint32_t counter_odd)
+{
+    for (int parity = 0; parity < 2; parity++) {
+        PassArgs a{c, parity, AlgoParams{param, seed, parity ? counter_odd : counter_even}, want_state};
+        int st = dispatch_gauge_algo<BatchedPass>(c->gauge, algo, a);
+        if (st) return st;
+        c->launches++;
+    }
+    return GF_OK;
+}
+
+int launch_quality(const gf_ctx *c, const CheckParams &cp)
+{
+    const unsigned blocks = (unsigned)c->total_qblocks;
+    const EngineDev e = c->dev();
+#define GFB_Q(G)                                                                                  \
+    if (cp.want_state == ST_FP32)                                                                 \
+        k_batched_quality<G, float, QNT><<<blocks, QNT, 0, c->stream>>>(e, c->total_qblocks, cp);  \
+    else                                                                                          \
+        k_batched_quality<G, double, QNT><<<blocks, QNT, 0, c->stream>>>(e, c->total_qblocks, cp);
+    switch (c->gauge) {
+    case LANDAU: GFB_Q(LANDAU) break;
+    case MAG: GFB_Q(MAG) break;
+    case U1XU1: GFB_Q(U1XU1) break;
+    default: GFB_Q(COULOMB) break;
+    }
+#undef GFB_Q
+    c->launches++;
+    return launch_status("batched quality");
+}
+
+int launch_reunitarise(const gf_ctx *c, int want_state, bool to64)
+{
+    const unsigned blocks = grid_for(c->total_links, 256);
+    if (to64)
+        k_reunitarise<float, true><<<blocks, 256, 0, c->stream>>>(c->dev(), c->total_links, want_state);
+    else if (want_state == ST_FP32)
+        k_reunitarise<float, false><<<blocks, 256, 0, c->stream>>>(c->dev(), c->total_links, want_state);
+    else
+        k_reunitarise<double, false><<<blocks, 256, 0, c->stream>>>(c->dev(), c->total_links, want_state);
+    c->launches++;
+    return launch_status("reunitarise");
+}
+
+int sync_states(gf_ctx *c)
+{
+    int st = cuda_status(cudaMemcpyAsync(c->h_state, c->d_state, sizeof(int) * 2 * c->ninst,
+                                         cudaMemcpyDeviceToHost, c->stream), "state copy");
+    if (st) return st;
+    return cuda_status(cudaStreamSynchronize(c->stream), "stream sync");
+}
+
+int check_ctx(gf_ctx *c)
+{
+    if (!c) {
+        set_error("context is NULL");
+        return GF_ERR_INVALID;
+    }
+    int dev = -1;
+    cudaGetDevice(&dev);
+    if (dev != c->device) {
+        int st = cuda_status(cudaSetDevice(c->device), "cudaSetDevice");
+        if (st) return st;
+    }
+    return GF_OK;
+}
+
+// One OR check chunk: nsweeps sweeps of the instances sweeping in FP32 (has32) and FP64
+// (has64), an optional reprojection, then the checks: FP64 first, then FP32 with the switch of
+// the instances that crossed switch_theta (so a switched instance is not counted twice).
+int enqueue_or_chunk(gf_ctx *c, int nsweeps, float omega, bool reproject, const CheckParams &base, bool has32,
+                     bool has64)
+{
+    int st = GF_OK;
+    for (int k = 0; k < nsweeps && !st; k++) {
+        if (has32) st = launch_sweep(c, ALG_OR, ST_FP32, omega, 0, 0, 0);
+        if (!st && has64) st = launch_sweep(c, ALG_OR, ST_FP64, omega, 0, 0, 0);
+    }
+    if (st) return st;
+    if (reproject) {
+        if (has32) st = launch_reunitarise(c, ST_FP32, false);
+        if (!st && has64) st = launch_reunitarise(c, ST_FP64, false);
+        if (st) return st;
+    }
+    CheckParams cp = base;
+    cp.chunk_sweeps = nsweeps;
+    cp.transitions = 1;
+    if (has64) {
+        cp.want_state = ST_FP64;
+        if ((st = launch_quality(c, cp))) return st;
+    }
+    if (has32) {
+        cp.want_state = ST_FP32;
+        if ((st = launch_quality(c, cp))) return st;
+        if ((st = launch_reunitarise(c, ST_SWITCH, true))) return st;
+        k_finish_switch<<<grid_for(c->ninst, 128), 128, 0, c->stream>>>(c->dev());
+        c->launches++;
+        st = launch_status("finish switch");
+    }
+    return st;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gf_create(const gf_ctx_params *p, gf_ctx **out)
+{
+    clear_error();
+    if (!p || !out || p->ninstances < 1 || !p->sizes || !valid_gauge(p->gauge)) {
+        set_error("invalid gf_ctx_params");
+        return GF_ERR_INVALID;
+    }
+    if (p->gauge == GF_COULOMB) {
+        set_error("GF_COULOMB contexts are not supported by the batched engine; use the plugin entry points");
+        return GF_ERR_UNSUPPORTED;
+    }
+    *out = nullptr;
+    gf_ctx *c = new (std::nothrow) gf_ctx();
+    if (!c) {
+        set_error("host allocation failed");
+        return GF_ERR_NOMEM;
+    }
+    c->gauge = p->gauge;
+    c->ninst = p->ninstances;
+    c->mixed = p->mixed ? 1 : 0;
+    cudaGetDevice(&c->device);
+    int st = GF_OK;
+    int64_t voff = 0, woff = 0, loff = 0, qoff = 0;
+    for (int i = 0; i < c->ninst && !st; i++) {
+        InstDesc d{};
+        st = make_geom(p->sizes + 4 * i, p->gauge, false, d.g);
+        d.warp_begin = woff;
+        d.link_begin = loff;
+        d.qblock_begin = qoff;
+        d.qblocks = (d.g.V + QNT - 1) / QNT;
+        // site offset: instances start on 128-byte boundaries of every plane (V is even, so
+        // rounding the offset up to 8 sites keeps float4 and double2 planes aligned)
+        d.f32 = reinterpret_cast<float4 *>(voff);  // rebased after allocation
+        d.f64 = reinterpret_cast<double2 *>(voff);
+        voff += 12 * ((d.g.V + 7) / 8 * 8);        // 4 mu x 3 float4 (or x 6 double2 -> x2)
+        woff += d.g.Vh / 8;
+        loff += 4 * d.g.V;
+        qoff += d.qblocks;
+        c->max_V = std::max(c->max_V, d.g.V);
+        c->h_inst.push_back(d);
+    }
+    if (st) {
+        delete c;
+        return st;
+    }
+    c->total_warps = woff;
+    c->total_links = loff;
+    c->total_qblocks = qoff;
+    const size_t n32 = (size_t)voff;   // float4 count
+    const size_t n64 = (size_t)voff * 2;  // double2 count
+    auto fail = [&](int s) {
+        gf_destroy(c);
+        return s;
+    };
+    if (p->stream) {
+        c->stream = (cudaStream_t)p->stream;
+    } else {
+        if ((st = cuda_status(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate")))
+            return fail(st);
+        c->own_stream = true;
+    }
+    if (c->mixed && (st = cuda_status(cudaMalloc(&c->f32, n32 * sizeof(float4)), "cudaMalloc FP32 field")))
+        return fail(st);
+    if ((st = cuda_status(cudaMalloc(&c->f64, n64 * sizeof(double2)), "cudaMalloc FP64 field"))) return fail(st);
+    for (auto &d : c->h_inst) {
+        const size_t off = (size_t)reinterpret_cast<uintptr_t>(d.f32);
+        d.f32 = c->mixed ? c->f32 + off : nullptr;
+        d.f64 = c->f64 + 2 * off;
+    }
+    const int n = c->ninst;
+    if ((st = cuda_status(cudaMalloc(&c->d_inst, sizeof(InstDesc) * n), "cudaMalloc"))) return fail(st);
+    if ((st = cuda_status(cudaMalloc(&c->d_state, sizeof(int) * 4 * n), "cudaMalloc"))) return fail(st);
+    c->d_storage = c->d_state + n;
+    c->d_sweeps = c->d_state + 2 * n;
+    c->d_sweeps64 = c->d_state + 3 * n;
+    if ((st = cuda_status(cudaMalloc(&c->d_quality, sizeof(double) * 2 * n), "cudaMalloc"))) return fail(st);
+    if ((st = cuda_status(cudaMalloc(&c->d_partials, sizeof(double) * 2 * c->total_qblocks), "cudaMalloc")))
+        return fail(st);
+    if ((st = cuda_status(cudaMalloc(&c->d_tickets, sizeof(unsigned) * n), "cudaMalloc"))) return fail(st);
+    if ((st = cuda_status(cudaHostAlloc(&c->h_state, sizeof(int) * 2 * n, cudaHostAllocDefault), "cudaHostAlloc")))
+        return fail(st);
+    if ((st = cuda_status(cudaHostAlloc(&c->h_quality, sizeof(double) * 2 * n, cudaHostAllocDefault),
+                          "cudaHostAlloc")))
+        return fail(st);
+    if ((st = cuda_status(cudaHostAlloc(&c->h_sweeps, sizeof(int) * 2 * n, cudaHostAllocDefault), "cudaHostAlloc")))
+        return fail(st);
+    for (int k = 0; k < 2; k++)
+        if ((st = cuda_status(cudaEventCreateWithFlags(&c->ev_chunk[k], cudaEventDisableTiming), "cudaEventCreate")))
+            return fail(st);
+    if ((st = cuda_status(cudaMemcpyAsync(c->d_inst, c->h_inst.data(), sizeof(InstDesc) * n, cudaMemcpyHostToDevice,
+                                          c->stream), "descriptor copy")))
+        return fail(st);
+    std::vector<int> init(4 * n, 0);
+    for (int i = 0; i < n; i++) {
+        init[i] = ST_DONE;                 // nothing imported yet
+        init[n + i] = c->mixed ? 0 : 1;    // storage
+    }
+    if ((st = cuda_status(cudaMemcpyAsync(c->d_state, init.data(), sizeof(int) * 4 * n, cudaMemcpyHostToDevice,
+                                          c->stream), "state init")))
+        return fail(st);
+    if ((st = cuda_status(cudaMemsetAsync(c->d_tickets, 0, sizeof(unsigned) * n, c->stream), "memset"))) return fail(st);
+    if ((st = cuda_status(cudaStreamSynchronize(c->stream), "sync"))) return fail(st);
+    *out = c;
+    return GF_OK;
+}
+
+int gf_destroy(gf_ctx *c)
+{
+    if (!c) return GF_OK;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    cudaFree(c->f32);
+    cudaFree(c->f64);
+    cudaFree(c->d_inst);
+    cudaFree(c->d_state);
+    cudaFree(c->d_quality);
+    cudaFree(c->d_partials);
+    cudaFree(c->d_tickets);
+    cudaFree(c->staging);
+    if (c->h_state) cudaFreeHost(c->h_state);
+    if (c->h_quality) cudaFreeHost(c->h_quality);
+    if (c->h_sweeps) cudaFreeHost(c->h_sweeps);
+    for (auto &e : c->ev_chunk)
+        if (e) cudaEventDestroy(e);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return GF_OK;
+}
+
+static int ensure_staging(gf_ctx *c, size_t bytes)
+{
+    if (c->staging_bytes >= bytes) return GF_OK;
+    cudaFree(c->staging);
+    c->staging = nullptr;
+    c->staging_bytes = 0;
+    int st = cuda_status(cudaMalloc(&c->staging, bytes), "cudaMalloc staging");
+    if (!st) c->staging_bytes = bytes;
+    return st;
+}
+
+int gf_import(gf_ctx *c, int instance, int real, const void *U, int on_host)
+{
+    clear_error();
+    int st = check_ctx(c);
+    if (st) return st;
+    if (instance < 0 || instance >= c->ninst || !U || !valid_real(real)) {
+        set_error("invalid instance, field or real type");
+        return GF_ERR_INVALID;
+    }
+    const InstDesc &d = c->h_inst[instance];
+    const size_t es = real == GF_FP64 ? 8 : 4;
+    const void *src = U;
+    if (on_host) {
+        // only the 12 planes of rows 0,1 of every mu travel (GpuPattern keeps them contiguous)
+        if ((st = ensure_staging(c, (size_t)d.g.V * 72 * es))) return st;
+        for (int mu = 0; mu < 4; mu++) {
+            const size_t off = (size_t)mu * 18 * d.g.V * es;
+            if ((st = cuda_status(cudaMemcpyAsync((char *)c->staging + off, (const char *)U + off, 12 * d.g.V * es,
+                                                  cudaMemcpyHostToDevice, c->stream), "H2D")))
+                return st;
+        }
+        src = c->staging;
+    }
+    const unsigned blocks = grid_for(4 * d.g.V, 256);
+    const int target = c->mixed ? ST_FP32 : ST_FP64;
+    if (target == ST_FP32) {
+        if (real == GF_FP64) k_import<double, float><<<blocks, 256, 0, c->stream>>>(c->dev(), instance, (const double *)src);
+        else k_import<float, float><<<blocks, 256, 0, c->stream>>>(c->dev(), instance, (const float *)src);
+    } else {
+        if (real == GF_FP64) k_import<double, double><<<blocks, 256, 0, c->stream>>>(c->dev(), instance, (const double *)src);
+        else k_import<float, double><<<blocks, 256, 0, c->stream>>>(c->dev(), instance, (const float *)src);
+    }
+    c->launches++;
+    if ((st = launch_status("import"))) return st;
+    const int z[2] = {0, 0};
+    const int stor = target == ST_FP32 ? 0 : 1;
+    if ((st = cuda_status(cudaMemcpyAsync(c->d_state + instance, &target, sizeof(int), cudaMemcpyHostToDevice,
+                                          c->stream), "state")))
+        return st;
+    if ((st = cuda_status(cudaMemcpyAsync(c->d_storage + instance, &stor, sizeof(int), cudaMemcpyHostToDevice,
+                                          c->stream), "storage")))
+        return st;
+    if ((st = cuda_status(cudaMemcpyAsync(c->d_sweeps + instance, z, sizeof(int), cudaMemcpyHostToDevice, c->stream),
+                          "sweeps")))
+        return st;
+    if ((st = cuda_status(cudaMemcpyAsync(c->d_sweeps64 + instance, z, sizeof(int), cudaMemcpyHostToDevice,
+                                          c->stream), "sweeps")))
+        return st;
+    return cuda_status(cudaStreamSynchronize(c->stream), "import sync");
+}
+
+// which field currently holds the instance
+static int storage_of(gf_ctx *c, int instance, int &st)
+{
+    st = sync_states(c);
+    return c->h_state[c->ninst + instance] == 0 ? GF_FP32 : GF_FP64;
+}
+
+int gf_export(gf_ctx *c, int instance, int real, void *U, int on_host)
+{
+    clear_error();
+    int st = check_ctx(c);
+    if (st) return st;
+    if (instance < 0 || instance >= c->ninst || !U || !valid_real(real)) {
+        set_error("invalid instance, field or real type");
+        return GF_ERR_INVALID;
+    }
+    const InstDesc &d = c->h_inst[instance];
+    const size_t es = real == GF_FP64 ? 8 : 4;
+    const int stor = storage_of(c, instance, st);
+    if (st) return st;
+    void *dst = U;
+    if (on_host) {
+        if ((st = ensure_staging(c, (size_t)d.g.V * 72 * es))) return st;
+        dst = c->staging;
+    }
+    const unsigned blocks = grid_for(4 * d.g.V, 256);
+    if (stor == GF_FP32) {
+        if (real == GF_FP64) k_export<float, double><<<blocks, 256, 0, c->stream>>>(c->dev(), instance, (double *)dst);
+        else k_export<float, float><<<blocks, 256, 0, c->stream>>>(c->dev(), instance, (float *)dst);
+    } else {
+        if (real == GF_FP64) k_export<double, double><<<blocks, 256, 0, c->stream>>>(c->dev(), instance, (double *)dst);
+        else k_export<double, float><<<blocks, 256, 0, c->stream>>>(c->dev(), instance, (float *)dst);
+    }
+    c->launches++;
+    if ((st = launch_status("export"))) return st;
+    if (on_host &&
+        (st = cuda_status(cudaMemcpyAsync(U, dst, (size_t)d.g.V * 72 * es, cudaMemcpyDeviceToHost, c->stream), "D2H")))
+        return st;
+    return cuda_status(cudaStreamSynchronize(c->stream), "export sync");
+}
+
+int gf_sweeps(gf_ctx *c, int algo, int nsweeps, float param, int seed, int rng_counter)
+{
+    clear_error();
+    int st = check_ctx(c);
+    if (st) return st;
+    if (algo < ALG_OR || algo > ALG_RANDOM || nsweeps < 0) {
+        set_error("invalid algorithm %d or sweep count %d", algo, nsweeps);
+        return GF_ERR_INVALID;
+    }
+    uint32_t ctr = (uint32_t)rng_counter;
+    for (int k = 0; k < nsweeps && !st; k++) {
+        // the reference takes a fresh Philox counter per launch (PhiloxWrapper::getNextCounter)
+        if (c->mixed) st = launch_sweep(c, algo, ST_FP32, param, (uint32_t)seed, ctr, ctr + 1);
+        if (!st) st = launch_sweep(c, algo, ST_FP64, param, (uint32_t)seed, ctr, ctr + 1);
+        ctr += 2;
+    }
+    return st;
+}
+
+int gf_reunitarize(gf_ctx *c)
+{
+    clear_error();
+    int st = check_ctx(c);
+    if (st) return st;
+    if (c->mixed && (st = launch_reunitarise(c, ST_FP32, false))) return st;
+    return launch_reunitarise(c, ST_FP64, false);
+}
+
+int gf_quality_all(gf_ctx *c, double *gff, double *theta)
+{
+    clear_error();
+    int st = check_ctx(c);
+    if (st) return st;
+    CheckParams cp{};
+    cp.stop_max = 0;
+    cp.transitions = 0;
+    if (c->mixed) {
+        cp.want_state = ST_FP32;
+        if ((st = launch_quality(c, cp))) return st;
+    }
+    cp.want_state = ST_FP64;
+    if ((st = launch_quality(c, cp))) return st;
+    if ((st = cuda_status(cudaMemcpyAsync(c->h_quality, c->d_quality, sizeof(double) * 2 * c->ninst,
+                                          cudaMemcpyDeviceToHost, c->stream), "quality copy")))
+        return st;
+    if ((st = cuda_status(cudaStreamSynchronize(c->stream), "sync"))) return st;
+    for (int i = 0; i < c->ninst; i++) {
+        if (gff) gff[i] = c->h_quality[2 * i];
+        if (theta) theta[i] = c->h_quality[2 * i + 1];
+    }
+    return GF_OK;
+}
+
+int gf_set_storage(gf_ctx *c, int real)
+{
+    clear_error();
+    int st = check_ctx(c);
+    if (st) return st;
+    if (!valid_real(real) || (real == GF_FP32 && !c->mixed)) {
+        set_error("FP32 storage needs a mixed context");
+        return GF_ERR_INVALID;
+    }
+    if (real == GF_FP64 && c->mixed) {
+        // FP32 -> FP64 with FP64 reunitarisation, as the mixed schedule does at the switch
+        std::vector<int> sw(c->ninst);
+        if ((st = sync_states(c))) return st;
+        for (int i = 0; i < c->ninst; i++) sw[i] = c->h_state[c->ninst + i] == 0 ? ST_SWITCH : c->h_state[i];
+        if ((st = cuda_status(cudaMemcpyAsync(c->d_state, sw.data(), sizeof(int) * c->ninst, cudaMemcpyHostToDevice,
+                                              c->stream), "state")))
+            return st;
+        if ((st = launch_reunitarise(c, ST_SWITCH, true))) return st;
+        k_finish_switch<<<grid_for(c->ninst, 128), 128, 0, c->stream>>>(c->dev());
+        if ((st = launch_status("finish switch"))) return st;
+        return sync_states(c);
+    }
+    return GF_OK;  // FP32 request on a mixed context: instances start in FP32 at import
+}
+
+int gf_fix(gf_ctx *c, const gf_schedule *s, gf_report *rep)
+{
+    clear_error();
+    int st = check_ctx(c);
+    if (st) return st;
+    if (!s || s->check_precision < 1 || s->reproject < 1 || s->or_max_iter < 0 || s->sa_steps < 0) {
+        set_error("invalid schedule");
+        return GF_ERR_INVALID;
+    }
+    uint32_t ctr = s->rng_counter;
+    // random gauge transformation of every instance (apps/LandauGaugeFixingSU3_4D.cu:192-196)
+    if (s->random_trafo) {
+        if ((st = gf_sweeps(c, ALG_RANDOM, 1, 0.f, (int)s->seed, (int)ctr))) return st;
+        ctr += 2;
+    }
+    // simulated annealing with microcanonical steps (:212-234); linear schedule as the
+    // reference, or geometric when sa_geometric is set
+    if (s->sa_steps > 0) {
+        float T = s->sa_max;
+        const float dT = (s->sa_max - s->sa_min) / (float)s->sa_steps;
+        const double ratio = s->sa_steps > 1 ? pow((double)s->sa_min / s->sa_max, 1.0 / (s->sa_steps - 1)) : 1.0;
+        for (int i = 0; i < s->sa_steps; i++) {
+            const float Ti = s->sa_geometric ? (float)(s->sa_max * pow(ratio, (double)i)) : T;
+            if ((st = gf_sweeps(c, ALG_SA, 1, Ti, (int)s->seed, (int)ctr))) return st;
+            ctr += 2;
+            if (s->micro_updates > 0 && (st = gf_sweeps(c, ALG_MICRO, s->micro_updates, 0.f, 0, 0))) return st;
+            if (i % s->reproject == 0 && (st = gf_reunitarize(c))) return st;
+            T -= dT;
+        }
+    }
+    // overrelaxation to theta < precision (:244-262).  The reference checks after sweep i when
+    // i % checkprecision == 0 (i = 0, C, 2C, ...) and reprojects when i % reproject == 0, so the
+    // first chunk is one sweep and the later ones C sweeps.  Every chunk shape is captured once
+    // as a CUDA graph and replayed; the host reads the states of chunk k-1 while chunk k runs.
+    CheckParams base{};
+    base.max_sweeps = s->or_max_iter;
+    base.switch_theta = c->mixed ? s->switch_theta : -1.0;
+    base.precision = s->precision;
+    base.stop_max = 0;
+    {
+        std::vector<int> zeros(2 * c->ninst, 0);
+        if ((st = cuda_status(cudaMemcpyAsync(c->d_sweeps, zeros.data(), sizeof(int) * 2 * c->ninst,
+                                              cudaMemcpyHostToDevice, c->stream), "sweeps reset")))
+            return st;
+    }
+    if ((st = sync_states(c))) return st;
+    const int C = s->check_precision;
+    struct Variant {
+        int n, repro, has32, has64;
+        cudaGraphExec_t exec;
+        long long nodes;
+    };
+    std::vector<Variant> graphs;
+    auto get_graph = [&](int n, int repro, int h32, int h64, cudaGraphExec_t &out) -> int {
+        for (auto &v : graphs)
+            if (v.n == n && v.repro == repro && v.has32 == h32 && v.has64 == h64) {
+                out = v.exec;
+                c->launches += v.nodes;
+                return GF_OK;
+            }
+        cudaGraph_t g = nullptr;
+        int r = cuda_status(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+        if (r) return r;
+        const long long before = c->launches;
+        r = enqueue_or_chunk(c, n, s->or_parameter, repro, base, h32, h64);
+        const long long nodes = c->launches - before;
+        const int r2 = cuda_status(cudaStreamEndCapture(c->stream, &g), "end capture");
+        if (r || r2) {
+            if (g) cudaGraphDestroy(g);
+            return r ? r : r2;
+        }
+        cudaGraphExec_t ex = nullptr;
+        r = cuda_status(cudaGraphInstantiate(&ex, g, 0), "graph instantiate");
+        cudaGraphDestroy(g);
+        if (r) return r;
+        graphs.push_back(Variant{n, repro, h32, h64, ex, nodes});
+        out = ex;
+        return GF_OK;
+    };
+    auto scan = [&](bool &any, bool &h32, bool &h64) {
+        any = h32 = h64 = false;
+        for (int i = 0; i < c->ninst; i++) {
+            const int q = c->h_state[i];
+            any |= q != ST_DONE;
+            h32 |= q == ST_FP32;
+            h64 |= q == ST_FP64 || q == ST_SWITCH;
+        }
+    };
+    bool any_active, has32, has64;
+    scan(any_active, has32, has64);
+    int issued = 0, launched = 0;
+    for (int k = 0; any_active && issued < s->or_max_iter && !st; k++) {
+        const int n = k == 0 ? 1 : std::min(C, s->or_max_iter - issued);
+        bool repro = false;
+        for (int i = issued; i < issued + n; i++) repro |= (i % s->reproject) == 0;
+        if (s->use_graphs) {
+            cudaGraphExec_t ex = nullptr;
+            if ((st = get_graph(n, repro, has32, has64, ex))) break;
+            if ((st = cuda_status(cudaGraphLaunch(ex, c->stream), "graph launch"))) break;
+        } else if ((st = enqueue_or_chunk(c, n, s->or_parameter, repro, base, has32, has64))) {
+            break;
+        }
+        issued += n;
+        if ((st = cuda_status(cudaMemcpyAsync(c->h_state, c->d_state, sizeof(int) * 2 * c->ninst,
+                                              cudaMemcpyDeviceToHost, c->stream), "state copy")))
+            break;
+        if ((st = cuda_status(cudaEventRecord(c->ev_chunk[k & 1], c->stream), "event"))) break;
+        launched++;
+        if (k >= 1) {
+            // pinned h_state holds the copy of chunk k-1 once its event has fired; the copy of
+            // chunk k lands later and is read in the next iteration
+            if ((st = cuda_status(cudaEventSynchronize(c->ev_chunk[(k - 1) & 1]), "event sync"))) break;
+            bool a2, h32b, h64b;
+            scan(a2, h32b, h64b);
+            any_active = a2;
+            has32 = h32b;
+            // an instance that switches to FP64 during chunk k is seen here after chunk k+1 was
+            // launched without FP64 passes: it idles for that chunk and is not counted for it
+            has64 = h64b;
+        }
+    }
+    for (auto &v : graphs) cudaGraphExecDestroy(v.exec);
+    if (st) return st;
+    if ((st = cuda_status(cudaStreamSynchronize(c->stream), "sync"))) return st;
+    if (rep) {
+        if ((st = cuda_status(cudaMemcpy(c->h_quality, c->d_quality, sizeof(double) * 2 * c->ninst,
+                                         cudaMemcpyDeviceToHost), "quality copy")))
+            return st;
+        if ((st = cuda_status(cudaMemcpy(c->h_sweeps, c->d_sweeps, sizeof(int) * 2 * c->ninst, cudaMemcpyDeviceToHost),
+                              "sweeps copy")))
+            return st;
+        if ((st = sync_states(c))) return st;
+        for (int i = 0; i < c->ninst; i++) {
+            rep[i].gff = c->h_quality[2 * i];
+            rep[i].theta = c->h_quality[2 * i + 1];
+            rep[i].or_sweeps = c->h_sweeps[i];
+            rep[i].or_sweeps_fp64 = c->h_sweeps[c->ninst + i];
+            rep[i].sa_sweeps = s->sa_steps;
+            rep[i].converged = rep[i].theta < s->precision;
+            rep[i].chunks = launched;
+        }
+    }
+    return GF_OK;
+}
+
+int gf_kernel_launches(gf_ctx *c, long long *count)
+{
+    if (!c || !count) {
+        set_error("NULL argument");
+        return GF_ERR_INVALID;
+    }
+    *count = c->launches;
+    return GF_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,224 @@
+// gf_engine.cuh -- batched kernels of the gauge-fixing engine: many lattices (gauge copies,
+// uneven extents) in one launch, each in the packed 12-real layout, with per-instance state so
+// converged instances drop out without host intervention.
+//
+// Instance state machine (one int per instance, written only by the quality / convert kernels
+// at the end of a check chunk):
+//   ST_FP32   sweeping on the FP32 field
+//   ST_SWITCH theta fell below the switch threshold; the convert kernel moves the field to FP64
+//   ST_FP64   sweeping on the FP64 field (FP64 polish, or plain FP64 runs)
+//   ST_DONE   converged (theta < precision) or out of sweeps
+#pragma once
+
+#include "gf_kernels.cuh"
+
+namespace gfb {
+
+enum InstState : int { ST_FP32 = 0, ST_FP64 = 1, ST_DONE = 2, ST_SWITCH = 3 };
+
+struct InstDesc {
+    Geom g;
+    int64_t warp_begin;   // first warp of this instance in a batched parity pass
+    int64_t link_begin;   // first link (s, mu) of this instance in a batched link kernel
+    int64_t qblock_begin; // first block of this instance in the batched quality kernel
+    int64_t qblocks;      // quality blocks of this instance
+    float4 *f32;          // packed FP32 field (may be null in plain-FP64 contexts)
+    double2 *f64;         // packed FP64 field
+};
+
+struct EngineDev {
+    const InstDesc *inst;
+    int ninst;
+    int *state;           // per instance
+    int *sweeps;          // per instance, sweeps done in the current phase machine
+    int *sweeps64;        // per instance, FP64 sweeps
+    int *storage;         // per instance: 0 = field lives in FP32, 1 = in FP64
+    double *quality;      // per instance: functional, theta
+    double *partials;     // per quality block: 2 doubles
+    unsigned int *tickets;// per instance
+};
+
+// index of the instance whose range [begin[i], begin[i+1]) holds x (ranges ascending)
+template <typename F>
+__device__ __forceinline__ int find_instance(const InstDesc *inst, int n, int64_t x, F begin_of)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (begin_of(inst[mid]) <= x)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+template <typename R>
+__device__ __forceinline__ PackedField<R> packed_of(const InstDesc &d);
+template <>
+__device__ __forceinline__ PackedField<float> packed_of<float>(const InstDesc &d) { return PackedField<float>{d.f32, d.g.V}; }
+template <>
+__device__ __forceinline__ PackedField<double> packed_of<double>(const InstDesc &d) { return PackedField<double>{d.f64, d.g.V}; }
+
+// One parity pass over every instance in state want_state.  A warp handles 8 sites of one
+// instance (instance ranges are whole warps).  seed_i = seed + instance, so instance 0 draws the
+// reference's Philox stream and the others draw independent ones.
+template <typename R, int GAUGE, int ALGO>
+__global__ void __launch_bounds__(128) k_batched_pass(EngineDev e, int64_t total_warps, int parity, AlgoParams p,
+                                                      int want_state)
+{
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (warp >= total_warps) return;
+    const int i = find_instance(e.inst, e.ninst, warp, [](const InstDesc &d) { return d.warp_begin; });
+    if (e.state[i] != want_state) return;
+    const InstDesc d = e.inst[i];
+    const PackedField<R> f = packed_of<R>(d);
+    AlgoParams pi = p;
+    pi.seed = p.seed + (uint32_t)i;
+    parity_pass_warp<R, GAUGE, ALGO>(f, f, d.g, warp - d.warp_begin, parity, pi);
+}
+
+// Quality of every instance in state want_state, with the state transitions of the check:
+//  ST_FP32 -> ST_SWITCH when theta < switch_theta (mixed runs), ST_FP64 -> ST_DONE when
+//  theta < precision; either -> ST_DONE when the sweep budget is spent.  chunk_sweeps is added
+//  to the instance's sweep count first.  Per-instance tickets make the last block of each
+//  instance reduce that instance's partials in block order (deterministic).
+struct CheckParams {
+    int want_state;
+    int chunk_sweeps;
+    int max_sweeps;
+    double switch_theta;  // <= 0: never switch
+    double precision;
+    int stop_max;
+    int transitions;      // 0: only measure
+};
+
+template <int GAUGE, typename R, int NT = 256>
+__global__ void __launch_bounds__(NT) k_batched_quality(EngineDev e, int64_t total_blocks, CheckParams cp)
+{
+    const int64_t b = blockIdx.x;
+    const int i = find_instance(e.inst, e.ninst, b, [](const InstDesc &d) { return d.qblock_begin; });
+    // with transitions: the instances sweeping in this precision; without: every instance whose
+    // field lives in this precision (uniform over the block)
+    if (cp.transitions ? (e.state[i] != cp.want_state) : (e.storage[i] != (sizeof(R) == 8 ? 1 : 0))) return;
+    const InstDesc d = e.inst[i];
+    const int64_t lb = b - d.qblock_begin;
+    const int64_t s = lb * NT + threadIdx.x;
+    double gv = 0, tv = 0;
+    if (s < d.g.V) quality_site<GAUGE, R>(packed_of<R>(d), d.g, s, gv, tv);
+    block_reduce2<NT>(gv, tv, cp.stop_max != 0);
+    __shared__ bool last;
+    if (threadIdx.x == 0) {
+        e.partials[2 * b] = gv;
+        e.partials[2 * b + 1] = tv;
+        __threadfence();
+        last = atomicAdd(&e.tickets[i], 1u) == (unsigned)d.qblocks - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double G = 0, T = 0;
+    for (int64_t k = threadIdx.x; k < d.qblocks; k += NT) {
+        G += __ldcg(&e.partials[2 * (d.qblock_begin + k)]);
+        const double t = __ldcg(&e.partials[2 * (d.qblock_begin + k) + 1]);
+        T = cp.stop_max ? fmax(T, t) : T + t;
+    }
+    block_reduce2<NT>(G, T, cp.stop_max != 0);
+    if (threadIdx.x == 0) {
+        const double gn = G * prefactor_gff_dev(GAUGE) / (double)d.g.V;
+        double tn = T * (1.0 / 3.0);
+        if (!cp.stop_max) tn = tn / (double)d.g.V;
+        e.quality[2 * i] = gn;
+        e.quality[2 * i + 1] = tn;
+        e.tickets[i] = 0;
+        if (cp.transitions) {
+            const int sw = e.sweeps[i] + cp.chunk_sweeps;
+            e.sweeps[i] = sw;
+            if (cp.want_state == ST_FP64) e.sweeps64[i] += cp.chunk_sweeps;
+            int st = cp.want_state;
+            if (st == ST_FP32 && cp.switch_theta > 0 && tn < cp.switch_theta) st = ST_SWITCH;
+            if (st == ST_FP64 && tn < cp.precision) st = ST_DONE;
+            if (sw >= cp.max_sweeps) st = ST_DONE;
+            e.state[i] = st;
+        }
+    }
+}
+
+// ---- link-wise kernels over all instances -----------------------------------------------------
+// import: reference GpuPattern (rows 0,1) -> packed field of type R
+template <typename Rin, typename R>
+__global__ void __launch_bounds__(256) k_import(EngineDev e, int i, const Rin *U)
+{
+    const InstDesc d = e.inst[i];
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= 4 * d.g.V) return;
+    const int mu = (int)(idx / d.g.V);
+    const int64_t s = idx - mu * d.g.V;
+    RefField<Rin> src{(Rin *)U, d.g.V};
+    Rin r[12];
+    src.load12(s, mu, r);
+    R o[12];
+#pragma unroll
+    for (int k = 0; k < 12; k++) o[k] = (R)r[k];
+    packed_of<R>(d).store12(s, mu, o);
+}
+
+// export: packed field of type R -> reference GpuPattern, reunitarised in FP64 with row 2
+// rebuilt (the reference's closing projectSU3, apps/LandauGaugeFixingSU3_4D.cu:271)
+template <typename R, typename Rout>
+__global__ void __launch_bounds__(256) k_export(EngineDev e, int i, Rout *U)
+{
+    const InstDesc d = e.inst[i];
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= 4 * d.g.V) return;
+    const int mu = (int)(idx / d.g.V);
+    const int64_t s = idx - mu * d.g.V;
+    Link<double> L;
+    load_link_f64<R>(packed_of<R>(d), s, mu, L);
+    project_rows(L);
+    Link<Rout> o;
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) o.e[a][b] = cx<Rout>((Rout)L.e[a][b].x, (Rout)L.e[a][b].y);
+    RefField<Rout>{U, d.g.V}.store18(s, mu, o);
+}
+
+// reunitarise (FP64 arithmetic) the packed field of every instance in state want_state; with
+// to64 = true, instances in ST_SWITCH are read from FP32 and written to FP64 instead
+template <typename R, bool TO64>
+__global__ void __launch_bounds__(256) k_reunitarise(EngineDev e, int64_t total_links, int want_state)
+{
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= total_links) return;
+    const int i = find_instance(e.inst, e.ninst, idx, [](const InstDesc &d) { return d.link_begin; });
+    if (e.state[i] != want_state) return;
+    const InstDesc d = e.inst[i];
+    const int64_t l = idx - d.link_begin;
+    const int mu = (int)(l / d.g.V);
+    const int64_t s = l - mu * d.g.V;
+    Link<double> L;
+    load_link_f64<R>(packed_of<R>(d), s, mu, L);
+    project_rows(L);
+    double r[12];
+    pack12(L, r);
+    if (TO64) {
+        packed_of<double>(d).store12(s, mu, r);
+    } else {
+        R o[12];
+#pragma unroll
+        for (int k = 0; k < 12; k++) o[k] = (R)r[k];
+        packed_of<R>(d).store12(s, mu, o);
+    }
+}
+
+__global__ void k_finish_switch(EngineDev e)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < e.ninst && e.state[i] == ST_SWITCH) {
+        e.state[i] = ST_FP64;
+        e.storage[i] = 1;
+    }
+}
+
+}  // namespace gfb

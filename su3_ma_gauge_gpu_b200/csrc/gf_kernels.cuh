@@ -7,6 +7,10 @@
 
 namespace gfb {
 
+// functional normalisation 1/(Nc*Nd), Coulomb 1/(Nc*(Nd-1)) (LandauKernelsSU3.hxx:79-82,
+// CoulombKernelsSU3.hxx:75-78); theta is normalised by 1/Nc
+__host__ __device__ constexpr double prefactor_gff_dev(int gauge) { return gauge == COULOMB ? 1.0 / 9.0 : 1.0 / 12.0; }
+
 // ---- one parity pass ---------------------------------------------------------------------------
 // 4 lanes per site (lane = 8*mu + site-in-warp), 8 sites per warp.  Vh is a multiple of 8 for
 // even extents, so a warp is either fully inside the parity half or fully outside.

@@ -1,0 +1,150 @@
+"""Batched, mixed-precision gauge fixing: the context-level C ABI from Python.
+
+:class:`GaugeFixer` holds one or more lattices (gauge copies, uneven extents)
+and runs the reference driver's per-copy schedule
+(apps/LandauGaugeFixingSU3_4D.cu:185-271: random trafo, SA + micro, OR with
+reprojection and checks) on all of them at once.  With ``mixed=True`` the bulk
+sweeps run in FP32 until theta < ``switch_theta``, then each instance moves to
+FP64 storage (reunitarised in FP64) for the polish to theta < ``precision``.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, fields
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, lib
+
+ALGOS = {"or": 0, "micro": 1, "sa": 2, "sr": 3, "random": 4}
+GAUGES = {"landau": _lib.GF_LANDAU, "mag": _lib.GF_MAG, "u1xu1": _lib.GF_U1XU1}
+
+
+@dataclass
+class Schedule:
+    """Fields of gf_schedule; defaults are the reference's ProgramOptions defaults
+    (apps/program_options/ProgramOptions.hxx:223-266) except where noted."""
+
+    random_trafo: int = 0
+    seed: int = 1
+    rng_counter: int = 0
+    sa_steps: int = 0
+    sa_min: float = 0.01
+    sa_max: float = 0.4
+    sa_geometric: int = 0
+    micro_updates: int = 3
+    or_max_iter: int = 1000
+    or_parameter: float = 1.7
+    precision: float = 1e-7
+    switch_theta: float = 1e-9
+    check_precision: int = 100
+    reproject: int = 100
+    use_graphs: int = 1
+
+    def to_c(self) -> _lib.Schedule:
+        s = _lib.Schedule()
+        for f in fields(self):
+            setattr(s, f.name, getattr(self, f.name))
+        return s
+
+
+@dataclass
+class Report:
+    gff: float
+    theta: float
+    or_sweeps: int
+    or_sweeps_fp64: int
+    sa_sweeps: int
+    converged: bool
+    chunks: int
+
+
+def _real(a) -> int:
+    dt = str(getattr(a, "dtype", ""))
+    if "float64" in dt:
+        return _lib.GF_FP64
+    if "float32" in dt:
+        return _lib.GF_FP32
+    raise TypeError(f"unsupported field dtype {dt}")
+
+
+class GaugeFixer:
+    """A gf_ctx: ``sizes`` is a list of (Nt, Nx, Ny, Nz), one per instance."""
+
+    def __init__(self, sizes, gauge="landau", mixed=True, stream=None):
+        self.sizes = [tuple(int(v) for v in s) for s in sizes]
+        self.gauge = GAUGES[gauge] if isinstance(gauge, str) else int(gauge)
+        arr = (ctypes.c_int32 * (4 * len(self.sizes)))(*[v for s in self.sizes for v in s])
+        self._keep = arr
+        p = _lib.CtxParams(self.gauge, len(self.sizes), ctypes.cast(arr, ctypes.POINTER(ctypes.c_int32)),
+                           1 if mixed else 0, stream.cuda_stream if stream is not None else None)
+        h = ctypes.c_void_p()
+        check(lib().gf_create(ctypes.byref(p), ctypes.byref(h)), "gf_create")
+        self._h = h
+        self.mixed = mixed
+
+    @property
+    def ninstances(self) -> int:
+        return len(self.sizes)
+
+    def load(self, i: int, U) -> None:
+        """Import instance i from a GpuPattern array: CUDA tensor, or numpy array (host)."""
+        if isinstance(U, np.ndarray):
+            U = np.ascontiguousarray(U)
+            check(lib().gf_import(self._h, i, _real(U), U.ctypes.data, 1), "gf_import")
+        else:
+            check(lib().gf_import(self._h, i, _real(U), U.data_ptr(), 0), "gf_import")
+
+    def store(self, i: int, U) -> None:
+        """Export instance i (reunitarised, row 2 rebuilt) into a GpuPattern array."""
+        if isinstance(U, np.ndarray):
+            assert U.flags.c_contiguous
+            check(lib().gf_export(self._h, i, _real(U), U.ctypes.data, 1), "gf_export")
+        else:
+            check(lib().gf_export(self._h, i, _real(U), U.data_ptr(), 0), "gf_export")
+
+    def sweeps(self, algo: str, n: int, param: float = 0.0, seed: int = 0, rng_counter: int = 0) -> None:
+        check(lib().gf_sweeps(self._h, ALGOS[algo], n, param, seed, rng_counter), "gf_sweeps")
+
+    def quality(self):
+        n = self.ninstances
+        g = (ctypes.c_double * n)()
+        a = (ctypes.c_double * n)()
+        check(lib().gf_quality_all(self._h, g, a), "gf_quality_all")
+        return np.array(g[:]), np.array(a[:])
+
+    def reunitarize(self) -> None:
+        check(lib().gf_reunitarize(self._h), "gf_reunitarize")
+
+    def to_fp64(self) -> None:
+        check(lib().gf_set_storage(self._h, _lib.GF_FP64), "gf_set_storage")
+
+    def fix(self, schedule: Schedule | None = None) -> list[Report]:
+        s = (schedule or Schedule()).to_c()
+        reps = (_lib.Report * self.ninstances)()
+        check(lib().gf_fix(self._h, ctypes.byref(s), reps), "gf_fix")
+        return [Report(r.gff, r.theta, r.or_sweeps, r.or_sweeps_fp64, r.sa_sweeps, bool(r.converged), r.chunks)
+                for r in reps]
+
+    def kernel_launches(self) -> int:
+        n = ctypes.c_longlong()
+        check(lib().gf_kernel_launches(self._h, ctypes.byref(n)), "gf_kernel_launches")
+        return n.value
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().gf_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

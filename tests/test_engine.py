@@ -1,0 +1,155 @@
+"""GPU tests of the context-level engine (packed layout, batching, mixed
+precision, device-side convergence) against the plugin-level path and the CPU
+oracle's whole-run driver."""
+import numpy as np
+import pytest
+
+import _oracle as O
+from su3_ma_gauge_gpu_b200 import synthetic as S
+
+pytestmark = pytest.mark.gpu
+
+
+def _plugin_sweeps(torch, U, size, algo, n, param=0.0, seed=0, counter=0, gauge=O.LANDAU):
+    """n sweeps through the plugin ABI on a reference-layout copy of U."""
+    import ctypes
+
+    from su3_ma_gauge_gpu_b200 import _lib
+
+    L = _lib.lib()
+    real = 1 if U.dtype == np.float64 else 0
+    dU = torch.from_numpy(U.copy()).cuda()
+    s = _lib.size_arg(size)
+    for k in range(n):
+        for parity in (0, 1):
+            c = counter + 2 * k + parity
+            if algo == "or":
+                st = L.gf_or_step(gauge, real, dU.data_ptr(), None, s, parity, ctypes.c_float(param), None)
+            elif algo == "micro":
+                st = L.gf_micro_step(gauge, real, dU.data_ptr(), None, s, parity, None)
+            elif algo == "sa":
+                st = L.gf_sa_step(gauge, real, dU.data_ptr(), None, s, parity, ctypes.c_float(param), seed, c, None)
+            else:
+                st = L.gf_random_trafo(gauge, real, dU.data_ptr(), None, s, parity, seed, c, None)
+            _lib.check(st, algo)
+    return dU
+
+
+def test_import_export_roundtrip(cuda):
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer
+
+    torch = cuda
+    size = (4, 4, 6, 8)
+    U, _ = S.smooth_config(size, 0.3, 5)
+    want = U.copy()
+    O.project(want, size)
+    for mixed in (False, True):
+        with GaugeFixer([size], mixed=mixed) as gf:
+            gf.load(0, U)  # host numpy path
+            out = np.zeros_like(U)
+            gf.store(0, out)
+            tol = 1e-14 if not mixed else 2e-7
+            assert np.abs(out - want).max() < tol
+            dU = torch.from_numpy(U).cuda()
+            gf.load(0, dU)  # device path
+            dout = torch.zeros_like(dU)
+            gf.store(0, dout)
+            assert np.abs(dout.cpu().numpy() - want).max() < tol
+
+
+@pytest.mark.parametrize("algo", ["or", "micro", "sa", "random"])
+def test_packed_sweeps_bit_identical_to_plugin_path(cuda, algo):
+    """Same kernel body, different HBM layout: FP64 results must agree bit for bit."""
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer
+
+    torch = cuda
+    size = (4, 6, 4, 8)
+    U, _ = S.smooth_config(size, 0.3, 8)
+    param = {"or": 1.7, "sa": 0.5}.get(algo, 0.0)
+    ref = _plugin_sweeps(torch, U, size, algo, 3, param, seed=3, counter=10).cpu().numpy()
+    with GaugeFixer([size], mixed=False) as gf:
+        gf.load(0, U)
+        gf.sweeps(algo, 3, param, seed=3, rng_counter=10)
+        g, a = gf.quality()
+        out = np.zeros_like(U)
+        gf.store(0, out)
+    want = ref.copy()
+    O.project(want, size)  # store() reunitarises like the reference's closing projectSU3
+    assert np.abs(out - want).max() < 1e-14
+    g_ref, a_ref = O.quality(ref, size, O.LANDAU)
+    assert g[0] == pytest.approx(g_ref, rel=1e-13)
+    assert a[0] == pytest.approx(a_ref, rel=1e-10)
+
+
+def test_batched_uneven_instances(cuda):
+    """Three lattices of different extents in one launch == each one on its own."""
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer
+
+    torch = cuda
+    sizes = [(4, 4, 4, 4), (2, 6, 4, 8), (6, 4, 2, 4)]
+    fields = [S.smooth_config(s, 0.3, 20 + i)[0] for i, s in enumerate(sizes)]
+    with GaugeFixer(sizes, mixed=False) as gf:
+        for i, U in enumerate(fields):
+            gf.load(i, U)
+        gf.sweeps("sa", 2, 0.7, seed=9, rng_counter=4)
+        gf.sweeps("or", 5, 1.7)
+        outs = []
+        for i, U in enumerate(fields):
+            o = np.zeros_like(U)
+            gf.store(i, o)
+            outs.append(o)
+    for i, (U, s) in enumerate(zip(fields, sizes)):
+        # instance i draws with seed + i
+        d = _plugin_sweeps(torch, U, s, "sa", 2, 0.7, seed=9 + i, counter=4)
+        ref = _plugin_sweeps(torch, d.cpu().numpy(), s, "or", 5, 1.7).cpu().numpy()
+        O.project(ref, s)
+        assert np.abs(outs[i] - ref).max() < 1e-13, i
+
+
+def _sched(**kw):
+    from su3_ma_gauge_gpu_b200.engine import Schedule
+
+    base = dict(or_max_iter=3000, precision=1e-11, check_precision=20, reproject=100, micro_updates=0)
+    base.update(kw)
+    return Schedule(**base)
+
+
+def test_fix_fp64_matches_oracle_driver(cuda):
+    """gf_fix (plain FP64) against the oracle's restatement of the Landau driver loop."""
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer
+
+    size = (4, 4, 4, 8)
+    U, _ = S.smooth_config(size, 0.3, 31)
+    sch = _sched(precision=1e-11, check_precision=10, reproject=50)
+    with GaugeFixer([size], mixed=False) as gf:
+        gf.load(0, U)
+        rep = gf.fix(sch)[0]
+        out = np.zeros_like(U)
+        gf.store(0, out)
+    ref = U.copy()
+    osch = O.Schedule(0, 0, 0.01, 0.4, 0, sch.or_max_iter, 1.7, sch.precision, sch.check_precision, sch.reproject, 1)
+    r, _ = O.fix(ref, size, O.LANDAU, osch)
+    assert rep.converged and rep.theta < 1e-11
+    assert rep.or_sweeps == r.or_iterations
+    assert rep.gff == pytest.approx(r.gff, rel=1e-12)
+    assert np.abs(out - ref).max() < 1e-9
+
+
+def test_fix_mixed_reaches_fp64_fixed_point(cuda):
+    """Mixed precision: FP32 bulk to 1e-9, FP64 polish to 1e-12; same functional as plain FP64."""
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer
+
+    size = (8, 8, 8, 8)
+    U, f0 = S.smooth_config(size, 0.3, 2)
+    res = {}
+    for mixed in (False, True):
+        with GaugeFixer([size], mixed=mixed) as gf:
+            gf.load(0, U)
+            rep = gf.fix(_sched(precision=1e-12, switch_theta=1e-9, check_precision=10))[0]
+            res[mixed] = rep
+    assert res[False].converged and res[True].converged
+    assert res[True].theta < 1e-12
+    assert 0 < res[True].or_sweeps_fp64 < res[True].or_sweeps
+    assert res[True].gff == pytest.approx(res[False].gff, rel=1e-10)
+    # the smooth field's untransformed functional is the maximum the fixing recovers
+    assert res[True].gff == pytest.approx(f0, rel=1e-2)

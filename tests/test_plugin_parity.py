@@ -6,8 +6,11 @@ both parity passes, on a random start):
   FP64: 1e-12 (OR / micro / SR / random trafo), 1e-11 (SA): the kernels sum the
         8 link quaternions in a shuffle tree and use CUDA's rsqrt/log/cospi, the
         oracle sums serially with libm; both round at the 1e-16 level.
-  FP32: 1e-5, the per-sweep bound the project is held to; MAG FP32 2e-4 because
-        g0 = D + sqrt(D^2+E^2+F^2) cancels on a random start.
+  FP32: 1e-5, the per-sweep bound the project is held to, on smooth
+        gauge-transformed fields (eps = 0.3), i.e. the inputs the gauge fixing
+        runs on.  On a random start the subgroup sums can cancel (U1xU1 keeps
+        only two components, MAG forms D + sqrt(D^2+E^2+F^2)), which amplifies
+        float rounding beyond any fixed bound; FP64 covers random starts.
 SA in FP32 is a rejection sampler: a last-bit difference can flip one accept
 decision, which changes that site completely; at most 1% of sites may do so.
 """
@@ -17,6 +20,7 @@ import numpy as np
 import pytest
 
 import _oracle as O
+from su3_ma_gauge_gpu_b200 import synthetic as S
 
 pytestmark = pytest.mark.gpu
 
@@ -72,8 +76,12 @@ def _cases():
 def test_sweep_matches_oracle(cuda, gauge, algo, size, dtype):
     torch = cuda
     real = 1 if dtype == np.float64 else 0
-    U = O.set_hot(size, 3, 1, dtype)
-    Udw = O.set_hot(size, 4, 1, dtype) if gauge == O.COULOMB else None
+    if dtype == np.float64:
+        U = O.set_hot(size, 3, 1, dtype)
+        Udw = O.set_hot(size, 4, 1, dtype) if gauge == O.COULOMB else None
+    else:
+        U = S.smooth_config(size, 0.3, 3, dtype=dtype)[0]
+        Udw = S.smooth_config(size, 0.3, 4, dtype=dtype)[0] if gauge == O.COULOMB else None
     G, Gdw = _gpu_sweep(torch, gauge, algo, U, Udw, size, real)
     for parity in (0, 1):
         O.step(U, size, gauge, algo, parity, _param(algo), 11, 7 + parity, Udw=Udw)
@@ -84,7 +92,7 @@ def test_sweep_matches_oracle(cuda, gauge, algo, size, dtype):
     if dtype == np.float64:
         tol = 1e-11 if algo == O.SA else 1e-12
     else:
-        tol = 2e-4 if gauge == O.MAG else 1e-5
+        tol = 1e-5
     if dtype == np.float32 and algo == O.SA:
         assert (err_site > tol).mean() <= 0.01, f"{(err_site > tol).sum()} of {V} sites differ"
     else:
