@@ -167,6 +167,27 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_profile_target(nsweeps: int):
+    """A short, fixed launch sequence of the hot kernels for ncu (see profiles/)."""
+    import torch
+
+    from su3_ma_gauge_gpu_b200 import synthetic as S
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer
+
+    U, _ = S.smooth_config(SIZE, EPS, 1234, device="cuda")
+    dU = torch.from_numpy(U).cuda()
+    with GaugeFixer([SIZE], mixed=True) as gf:
+        gf.load(0, dU)
+        gf.sweeps("or", nsweeps, 1.7)
+        gf.to_fp64()
+        gf.sweeps("or", nsweeps, 1.7)
+        g, a = gf.quality()
+        gf.store(0, dU)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_target": "ok", "sweeps_per_precision": nsweeps, "F": float(g[0]),
+                      "theta": float(a[0])}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -176,9 +197,15 @@ def main():
     ap.add_argument("--check", type=int, default=20, help="sweeps between quality checks")
     ap.add_argument("--cpu-budget", type=float, default=10.0)
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison run")
+    ap.add_argument("--profile", type=int, default=0, metavar="N",
+                    help="profiling target: import the 32^4 input, N FP32 OR sweeps, switch to FP64, N FP64 "
+                         "sweeps, one quality check; no timing output")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.profile:
+        run_profile_target(args.profile)
         return
 
     import numpy as np

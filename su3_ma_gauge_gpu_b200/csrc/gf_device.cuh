@@ -179,7 +179,7 @@ __device__ __forceinline__ float Rng<float>::rand()
         local--;
     }
     const uint32_t v = local == 3 ? res.w : (local == 2 ? res.z : (local == 1 ? res.y : res.x));
-    return (float)(1u + (v >> 8)) * 5.96046412226771e-08f;  // 0x1.fffffep-25f
+    return (float)(1u + (v >> 8)) * 0x1.fffffep-25f;
 }
 
 template <>
@@ -193,7 +193,7 @@ __device__ __forceinline__ double Rng<double>::rand()
         local--;
     }
     const uint64_t v = local == 1 ? (((uint64_t)res.w << 32) | res.z) : (((uint64_t)res.y << 32) | res.x);
-    return (double)(1ull + (v >> 11)) * 1.1102230246251564e-16;  // 0x1.fffffffffffffp-54
+    return (double)(1ull + (v >> 11)) * 0x1.fffffffffffffp-54;
 }
 
 // ---- update rules on the accumulated 4-vector (gaugefixing/algorithms/*Update.hxx) ----------
@@ -397,29 +397,67 @@ __device__ __forceinline__ void site_update(Link<R> &up, Link<R> &dn, int mu, co
 }
 
 // ---- lattice geometry -----------------------------------------------------------------------
+// Division by a lattice extent without a divide instruction: for 0 <= n < 2^31 and d >= 1,
+// q = (umulhi(n, m) + n) >> s with s = ceil(log2 d), m = floor(2^32 (2^s - d) / d) + 1
+// (Granlund & Montgomery, "Division by invariant integers using multiplication", PLDI 1994).
+struct FastDiv {
+    uint32_t d, m, s;
+    __host__ __device__ __forceinline__ uint32_t div(uint32_t n) const { return (__umulhi_any(n, m) + n) >> s; }
+
+  private:
+    __host__ __device__ static __forceinline__ uint32_t __umulhi_any(uint32_t a, uint32_t b)
+    {
+#ifdef __CUDA_ARCH__
+        return __umulhi(a, b);
+#else
+        return (uint32_t)(((uint64_t)a * b) >> 32);
+#endif
+    }
+};
+
+inline FastDiv make_fastdiv(uint32_t d)
+{
+    uint32_t s = 0;
+    while ((1ull << s) < d) s++;
+    const uint64_t m = ((uint64_t(1) << 32) * ((uint64_t(1) << s) - d)) / d + 1;
+    return FastDiv{d, (uint32_t)m, s};
+}
+
 // Parity-split site order of the reference (SiteCoord.hxx:104-175): lexicographic l =
-// ((t*Nx + x)*Ny + y)*Nz + z, s = l/2 (+V/2 for odd t+x+y+z).  All extents must be even.
+// ((t*Nx + x)*Ny + y)*Nz + z, s = l/2 (+V/2 for odd t+x+y+z).  All extents must be even and
+// V < 2^31, so site arithmetic is 32-bit.
 struct Geom {
     int32_t n[4];   // Nt, Nx, Ny, Nz
     int64_t V, Vh;
+    FastDiv dx, dy, dz;
 };
 
-__device__ __forceinline__ void site_coords(const Geom &g, int64_t h, int parity, int32_t c[4])
+inline void geom_init_div(Geom &g)
 {
-    int64_t l = 2 * h;
-    c[3] = (int32_t)(l % g.n[3]);
-    l /= g.n[3];
-    c[2] = (int32_t)(l % g.n[2]);
-    l /= g.n[2];
-    c[1] = (int32_t)(l % g.n[1]);
-    c[0] = (int32_t)(l / g.n[1]);
+    g.dx = make_fastdiv((uint32_t)g.n[1]);
+    g.dy = make_fastdiv((uint32_t)g.n[2]);
+    g.dz = make_fastdiv((uint32_t)g.n[3]);
+}
+
+__device__ __forceinline__ void site_coords(const Geom &g, int64_t h64, int parity, int32_t c[4])
+{
+    uint32_t l = 2u * (uint32_t)h64;
+    uint32_t q = g.dz.div(l);
+    c[3] = (int32_t)(l - q * g.dz.d);
+    l = q;
+    q = g.dy.div(l);
+    c[2] = (int32_t)(l - q * g.dy.d);
+    l = q;
+    q = g.dx.div(l);
+    c[1] = (int32_t)(l - q * g.dx.d);
+    c[0] = (int32_t)q;
     if (((c[0] + c[1] + c[2] + c[3]) & 1) != parity) c[3] += 1;
 }
 
 __device__ __forceinline__ int64_t site_index(const Geom &g, const int32_t c[4])
 {
-    const int64_t l = (((int64_t)c[0] * g.n[1] + c[1]) * g.n[2] + c[2]) * g.n[3] + c[3];
-    return (l >> 1) + (((c[0] + c[1] + c[2] + c[3]) & 1) ? g.Vh : 0);
+    const uint32_t l = (((uint32_t)c[0] * g.n[1] + c[1]) * g.n[2] + c[2]) * g.n[3] + c[3];
+    return (int64_t)(l >> 1) + (((c[0] + c[1] + c[2] + c[3]) & 1) ? g.Vh : 0);
 }
 
 // backward neighbour x - mu of the site with coordinates c (mu is lane-dependent, so the

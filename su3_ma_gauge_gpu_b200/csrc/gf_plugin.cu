@@ -58,6 +58,7 @@ int make_geom(const int32_t size[4], int gauge, bool plugin_slice, Geom &g)
     }
     g.V = V;
     g.Vh = V / 2;
+    geom_init_div(g);
     return GF_OK;
 }
 

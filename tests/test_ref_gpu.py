@@ -1,0 +1,222 @@
+"""Parity with the reference's OWN CUDA kernels, run on the same GPU.
+
+oracle/Makefile compiles the reference's plugin classes (gaugefixing/*KernelsSU3.hxx,
+CommonKernelsSU3, GaugeFixingStats) for sm_100a with the reference's flags
+(-use_fast_math -Xptxas -dlcm=cg) and compile-time extents 4^3 x 8 (oracle/_ref/).
+Each case runs one sweep (both parities) of the same input through the
+reference kernels and through this library's plugin ABI.
+
+Tolerances: FP64 1e-12 per sweep (the reference sums serially, this library in
+a shuffle tree; both use CUDA's rsqrt).  FP32 on smooth fields: overrelaxation
+1e-5 per sweep against the reference kernels; every update at least as
+accurate as the reference's FP32 kernels (shared-memory atomics in arbitrary
+order, -use_fast_math), both measured against the FP64 oracle on the same
+input: error <= max(1e-5, 4 x the reference's).  SA in FP32: at most 5% of
+sites may take a different accept/reject path.
+
+The 32^4 Landau OR timing of the reference kernels (the on-box GPU baseline)
+is recorded by test_reference_kernel_timing; set GF_REF_TIMING_OUT to a file
+name to keep the numbers.
+"""
+import ctypes
+import json
+import os
+
+import numpy as np
+import pytest
+
+import _oracle as O
+from su3_ma_gauge_gpu_b200 import synthetic as S
+
+pytestmark = pytest.mark.gpu
+
+REF = O.REF_DIR
+
+
+def _reflib(name):
+    p = REF / name
+    if not p.exists():
+        pytest.skip(f"{p.name} not built (reference tree absent when oracle/ was built)")
+    lib = ctypes.CDLL(str(p))
+    lib.refgpu_step.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                ctypes.c_int, ctypes.c_float, ctypes.c_int, ctypes.c_int]
+    lib.refgpu_quality.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                   ctypes.POINTER(ctypes.c_double)]
+    return lib
+
+
+def _config(lib):
+    size = (ctypes.c_int * 4)()
+    es = lib.refgpu_config(size)
+    return tuple(size), es
+
+
+def _nn(torch, lib, size, timeslice):
+    V = int(np.prod(size)) if not timeslice else int(np.prod(size[1:]))
+    nn = np.zeros(8 * V, np.int32)
+    lib.refgpu_neighbour_table(timeslice, nn.ctypes.data_as(ctypes.c_void_p))
+    return torch.from_numpy(nn).cuda()
+
+
+def _ours(torch, gauge, algo, U, Udw, size, real, param, seed, counter):
+    from su3_ma_gauge_gpu_b200 import _lib
+
+    L = _lib.lib()
+    s = _lib.size_arg(size)
+    dU = torch.from_numpy(U.copy()).cuda()
+    dD = torch.from_numpy(Udw.copy()).cuda() if Udw is not None else None
+    for parity in (0, 1):
+        a = (gauge, real, dU.data_ptr(), dD.data_ptr() if dD is not None else None, s, parity)
+        if algo == 0:
+            st = L.gf_or_step(*a, ctypes.c_float(param), None)
+        elif algo == 1:
+            st = L.gf_micro_step(*a, None)
+        elif algo == 2:
+            st = L.gf_sa_step(*a, ctypes.c_float(param), seed, counter + parity, None)
+        elif algo == 3:
+            st = L.gf_sr_step(*a, ctypes.c_float(param), seed, counter + parity, None)
+        else:
+            st = L.gf_random_trafo(*a, seed, counter + parity, None)
+        _lib.check(st, "step")
+    torch.cuda.synchronize()
+    return dU.cpu().numpy(), (dD.cpu().numpy() if dD is not None else None)
+
+
+CASES = [(g, a) for g in (O.LANDAU, O.COULOMB, O.MAG, O.U1XU1) for a in (0, 1, 2, 3, 4)
+         if not (a == 3 and g != O.MAG)]
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("gauge,algo", CASES)
+def test_sweep_matches_reference_kernels(cuda, gauge, algo, prec):
+    torch = cuda
+    lib = _reflib(f"libref_gpu_{'u1_' if gauge == O.U1XU1 else ''}X4T8_{prec}.so")
+    full, es = _config(lib)
+    dtype = np.float64 if prec == "f64" else np.float32
+    assert es == np.dtype(dtype).itemsize
+    size = (1,) + full[1:] if gauge == O.COULOMB else full
+    if prec == "f64":
+        U = O.set_hot(size, 13, 2, dtype)
+        Udw = O.set_hot(size, 14, 2, dtype) if gauge == O.COULOMB else None
+    else:
+        U = S.smooth_config(size, 0.3, 13, dtype=dtype)[0]
+        Udw = S.smooth_config(size, 0.3, 14, dtype=dtype)[0] if gauge == O.COULOMB else None
+    param = {0: 1.7, 2: 0.6, 3: 0.5}.get(algo, 0.0)
+    nn = _nn(torch, lib, full, gauge == O.COULOMB)
+    rU = torch.from_numpy(U.copy()).cuda()
+    rD = torch.from_numpy(Udw.copy()).cuda() if Udw is not None else None
+    for parity in (0, 1):
+        rc = lib.refgpu_step(gauge, algo, rU.data_ptr(), rD.data_ptr() if rD is not None else None, nn.data_ptr(),
+                             parity, param, 5, 40 + parity)
+        assert rc == 0
+    torch.cuda.synchronize()
+    G, Gd = _ours(torch, gauge, algo, U, Udw, size, 1 if prec == "f64" else 0, param, 5, 40)
+    V = int(np.prod(size))
+    a = rU.cpu().numpy().reshape(4, 3, 3, 2, V)[:, :2].astype(np.float64)
+    b = G.reshape(4, 3, 3, 2, V)[:, :2].astype(np.float64)
+    assert np.abs(a - U.reshape(4, 3, 3, 2, V)[:, :2]).max() > 1e-4  # the sweep did something
+    err_site = np.abs(a - b).max(axis=(0, 1, 2, 3))
+    tol = (1e-11 if algo == 2 else 1e-12) if prec == "f64" else 1e-5
+    if prec == "f64":
+        assert err_site.max() < tol, f"max err {err_site.max():.3e}"
+    elif algo == 2:
+        assert (err_site > tol).mean() <= 0.05
+    else:
+        if algo == 0:
+            assert err_site.max() < tol, f"max err vs reference kernels {err_site.max():.3e}"
+        X = U.astype(np.float64)
+        Xdw = None if Udw is None else Udw.astype(np.float64)
+        for parity in (0, 1):
+            O.step(X, size, gauge, algo, parity, param, 5, 40 + parity, Udw=Xdw)
+        ex = X.reshape(4, 3, 3, 2, V)[:, :2]
+        err_ours, err_ref = np.abs(b - ex).max(), np.abs(a - ex).max()
+        assert err_ours <= max(tol, 4 * err_ref), f"ours {err_ours:.3e} vs reference kernels {err_ref:.3e}"
+    if rD is not None and not (prec == "f32" and algo == 2):
+        d = np.abs(rD.cpu().numpy().reshape(4, 3, 3, 2, V)[:, :2] - Gd.reshape(4, 3, 3, 2, V)[:, :2]).max()
+        assert d < (tol if prec == "f64" else 4e-5)
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("gauge", [O.LANDAU, O.COULOMB, O.MAG, O.U1XU1])
+def test_quality_matches_reference_stats(cuda, gauge, prec):
+    from su3_ma_gauge_gpu_b200 import GaugeFixingStats
+
+    torch = cuda
+    lib = _reflib(f"libref_gpu_{'u1_' if gauge == O.U1XU1 else ''}X4T8_{prec}.so")
+    full, _ = _config(lib)
+    dtype = np.float64 if prec == "f64" else np.float32
+    size = (1,) + full[1:] if gauge == O.COULOMB else full
+    U = S.smooth_config(size, 0.3, 17, dtype=dtype)[0]
+    dU = torch.from_numpy(U).cuda()
+    g, a = ctypes.c_double(), ctypes.c_double()
+    assert lib.refgpu_quality(gauge, dU.data_ptr(), ctypes.byref(g), ctypes.byref(a)) == 0
+
+    class G:
+        GAUGE = gauge
+
+    st = GaugeFixingStats(dU, size, G, "AVERAGE", precision="double" if prec == "f64" else "float")
+    st.generateGaugeQuality()
+    # the reference computes the per-site terms in Real (float with -use_fast_math for FP32), this
+    # library in FP64 from the stored rows
+    rel = 1e-12 if prec == "f64" else 1e-5
+    assert st.getCurrentGff() == pytest.approx(g.value, rel=rel)
+    assert st.getCurrentA() == pytest.approx(a.value, rel=rel if prec == "f64" else 1e-4)
+
+
+def test_reference_kernel_timing(cuda):
+    """32^4 Landau OR sweep: the reference kernels (sm_100a build) vs this library, same GPU."""
+    from su3_ma_gauge_gpu_b200 import _lib
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer
+
+    torch = cuda
+    out = {}
+    size = (32, 32, 32, 32)
+    V = int(np.prod(size))
+    U, _ = S.smooth_config(size, 0.3, 1234, device="cuda")
+    for prec, dt, nb in (("f32", np.float32, 4), ("f64", np.float64, 8)):
+        lib = _reflib(f"libref_gpu_X32T32_{prec}.so")
+        dU = torch.from_numpy(U.astype(dt)).cuda()
+        nn = _nn(torch, lib, size, 0)
+
+        def ref_sweep():
+            for p in (0, 1):
+                lib.refgpu_step(0, 0, dU.data_ptr(), None, nn.data_ptr(), p, 1.7, 0, 0)
+
+        def time_it(fn, n=20, stream=None):
+            for _ in range(3):
+                fn()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for _ in range(n):
+                fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) / n
+
+        t_ref = time_it(ref_sweep)
+        L = _lib.lib()
+        s = _lib.size_arg(size)
+        real = 1 if prec == "f64" else 0
+
+        def plugin_sweep():
+            for p in (0, 1):
+                L.gf_or_step(0, real, dU.data_ptr(), None, s, p, ctypes.c_float(1.7), None)
+
+        t_plugin = time_it(plugin_sweep)
+        stream = torch.cuda.Stream()
+        gf = GaugeFixer([size], mixed=(prec == "f32"), stream=stream)
+        gf.load(0, dU)
+        torch.cuda.synchronize()
+        t_packed = time_it(lambda: gf.sweeps("or", 1, 1.7), stream=stream)
+        gf.close()
+        gbs = lambda t: 192 * nb * V / (t * 1e-3) / 1e9  # noqa: E731
+        out[prec] = {"ref_ms_per_sweep": t_ref, "ref_GBs": gbs(t_ref), "plugin_ms_per_sweep": t_plugin,
+                     "plugin_GBs": gbs(t_plugin), "packed_ms_per_sweep": t_packed, "packed_GBs": gbs(t_packed),
+                     "speedup_packed_vs_ref": t_ref / t_packed}
+    print(json.dumps(out))
+    path = os.environ.get("GF_REF_TIMING_OUT")
+    if path:
+        with open(path, "w") as f:
+            json.dump(out, f, indent=1)
+    assert out["f64"]["packed_ms_per_sweep"] > 0
