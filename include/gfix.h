@@ -138,6 +138,7 @@ typedef struct gf_schedule {
     int check_precision;   /* checkprecision: sweeps between checks */
     int reproject;         /* reproject: sweeps between reunitarisations */
     int use_graphs;        /* 1: replay check chunks from CUDA graphs */
+    int autotune;          /* 1: gf_autotune first if the context is not tuned yet */
 } gf_schedule;
 
 typedef struct gf_report {
@@ -168,6 +169,13 @@ int gf_reunitarize(gf_ctx *ctx);
 int gf_set_storage(gf_ctx *ctx, int real);
 /* The whole per-copy schedule for all instances; reports has ninstances entries (or NULL). */
 int gf_fix(gf_ctx *ctx, const gf_schedule *schedule, gf_report *reports);
+/* Autotuner: times the candidate launch shapes of the OR parity pass (one warp per 8-site tile;
+ * pipelined with cp.async prefetch and 2, 4 or 8 warps per block) on a scratch copy of the
+ * field and keeps the fastest per precision.  Outputs: 0 = direct, else warps per block of the
+ * pipelined pass (-1: precision not used). */
+int gf_autotune(gf_ctx *ctx, int *choice_fp32, int *choice_fp64);
+/* Fix the launch shape instead: variant 0 (direct) or 1 (pipelined, warps = 2, 4 or 8). */
+int gf_set_pass_shape(gf_ctx *ctx, int real, int variant, int warps);
 /* Number of kernels this context has launched so far (each node of a replayed graph counts). */
 int gf_kernel_launches(gf_ctx *ctx, long long *count);
 

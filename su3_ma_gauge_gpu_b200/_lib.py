@@ -64,7 +64,8 @@ class Schedule(ctypes.Structure):
                 ("sa_steps", ctypes.c_int), ("sa_min", ctypes.c_float), ("sa_max", ctypes.c_float),
                 ("sa_geometric", ctypes.c_int), ("micro_updates", ctypes.c_int), ("or_max_iter", ctypes.c_int),
                 ("or_parameter", ctypes.c_float), ("precision", ctypes.c_double), ("switch_theta", ctypes.c_double),
-                ("check_precision", ctypes.c_int), ("reproject", ctypes.c_int), ("use_graphs", ctypes.c_int)]
+                ("check_precision", ctypes.c_int), ("reproject", ctypes.c_int), ("use_graphs", ctypes.c_int),
+                ("autotune", ctypes.c_int)]
 
 
 class Report(ctypes.Structure):
@@ -86,6 +87,8 @@ SIGNATURES.update({
     "gf_set_storage": (_c_int, [_vp, _c_int]),
     "gf_fix": (_c_int, [_vp, ctypes.POINTER(Schedule), ctypes.POINTER(Report)]),
     "gf_kernel_launches": (_c_int, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
+    "gf_autotune": (_c_int, [_vp, ctypes.POINTER(_c_int), ctypes.POINTER(_c_int)]),
+    "gf_set_pass_shape": (_c_int, [_vp, _c_int, _c_int, _c_int]),
 })
 
 _LIB = None

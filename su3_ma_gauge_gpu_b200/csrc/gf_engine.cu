@@ -39,6 +39,14 @@ struct gf_ctx {
     size_t staging_bytes = 0;
     cudaEvent_t ev_chunk[2] = {nullptr, nullptr};
     mutable long long launches = 0;  // kernels this context has launched (graph nodes per replay)
+    int num_sms = 148;
+    // parity-pass launch shape per precision ([0] FP32, [1] FP64): variant 0 = one warp per
+    // 8-site tile, 128 threads per block; variant 1 = pipelined (cp.async prefetch of the next
+    // tile), `warps` warps per block, grid = num_sms * blocks_per_sm
+    struct PassShape {
+        int variant = 0, warps = 4, blocks_per_sm = 0;
+    } shape[2];
+    int tuned[2] = {0, 0};
 
     EngineDev dev() const
     {
@@ -70,31 +78,66 @@ struct PassArgs {
     int want_state;
 };
 
+template <typename R, int GAUGE, int ALGO, int WARPS>
+int launch_staged(const gf_ctx *c, const EngineDev &e, const PassArgs &a, int blocks_per_sm)
+{
+    const size_t smem = staged_smem_bytes<R>(WARPS);
+    auto kern = k_batched_pass_staged<R, GAUGE, ALGO, WARPS>;
+    int occ = blocks_per_sm;
+    if (occ <= 0) {
+        int o = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, WARPS * 32, smem) != cudaSuccess || o < 1) o = 1;
+        occ = o;
+    }
+    const int64_t need = (a.c->total_warps + WARPS - 1) / WARPS;
+    const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)c->num_sms * occ));
+    kern<<<blocks, WARPS * 32, smem, a.c->stream>>>(e, a.c->total_warps, a.parity, a.p, a.want_state);
+    return launch_status("batched parity pass (pipelined)");
+}
+
+template <typename R, int GAUGE, int ALGO>
+int launch_pass(const gf_ctx *c, const EngineDev &e, const PassArgs &a, const gf_ctx::PassShape &sh)
+{
+    if constexpr (ALGO == ALG_OR) {
+        if (sh.variant == 1) {
+            switch (sh.warps) {
+            case 2: return launch_staged<R, GAUGE, ALGO, 2>(c, e, a, sh.blocks_per_sm);
+            case 8: return launch_staged<R, GAUGE, ALGO, 8>(c, e, a, sh.blocks_per_sm);
+            default: return launch_staged<R, GAUGE, ALGO, 4>(c, e, a, sh.blocks_per_sm);
+            }
+        }
+    }
+    const unsigned blocks = grid_for(a.c->total_warps * 32, 128);
+    k_batched_pass<R, GAUGE, ALGO><<<blocks, 128, 0, a.c->stream>>>(e, a.c->total_warps, a.parity, a.p,
+                                                                     a.want_state);
+    return launch_status("batched parity pass");
+}
+
 template <int GAUGE, int ALGO>
 struct BatchedPass {
-    static int run(const PassArgs &a)
+    static int run(const PassArgs &a, const EngineDev &e, const gf_ctx::PassShape *shape)
     {
-        const unsigned blocks = grid_for(a.c->total_warps * 32, 128);
-        if (a.want_state == ST_FP32)
-            k_batched_pass<float, GAUGE, ALGO><<<blocks, 128, 0, a.c->stream>>>(a.c->dev(), a.c->total_warps,
-                                                                             a.parity, a.p, a.want_state);
-        else
-            k_batched_pass<double, GAUGE, ALGO><<<blocks, 128, 0, a.c->stream>>>(a.c->dev(), a.c->total_warps,
-                                                                              a.parity, a.p, a.want_state);
-        return launch_status("batched parity pass");
+        if (a.want_state == ST_FP32) return launch_pass<float, GAUGE, ALGO>(a.c, e, a, shape[0]);
+        return launch_pass<double, GAUGE, ALGO>(a.c, e, a, shape[1]);
     }
 };
 
-int launch_sweep(const gf_ctx *c, int algo, int want_state, float param, uint32_t seed, uint32_t counter_even,
-                 uint32_t counter_odd)
+int launch_sweep_on(const gf_ctx *c, const EngineDev &e, const gf_ctx::PassShape *shape, int algo, int want_state,
+                    float param, uint32_t seed, uint32_t counter_even, uint32_t counter_odd)
 {
     for (int parity = 0; parity < 2; parity++) {
         PassArgs a{c, parity, AlgoParams{param, seed, parity ? counter_odd : counter_even}, want_state};
-        int st = dispatch_gauge_algo<BatchedPass>(c->gauge, algo, a);
+        int st = dispatch_gauge_algo<BatchedPass>(c->gauge, algo, a, e, shape);
         if (st) return st;
         c->launches++;
     }
     return GF_OK;
+}
+
+int launch_sweep(const gf_ctx *c, int algo, int want_state, float param, uint32_t seed, uint32_t counter_even,
+                 uint32_t counter_odd)
+{
+    return launch_sweep_on(c, c->dev(), c->shape, algo, want_state, param, seed, counter_even, counter_odd);
 }
 
 int launch_quality(const gf_ctx *c, const CheckParams &cp)
@@ -213,6 +256,7 @@ int gf_create(const gf_ctx_params *p, gf_ctx **out)
     c->ninst = p->ninstances;
     c->mixed = p->mixed ? 1 : 0;
     cudaGetDevice(&c->device);
+    cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device);
     int st = GF_OK;
     int64_t voff = 0, woff = 0, loff = 0, qoff = 0;
     for (int i = 0; i < c->ninst && !st; i++) {
@@ -510,6 +554,8 @@ int gf_fix(gf_ctx *c, const gf_schedule *s, gf_report *rep)
         set_error("invalid schedule");
         return GF_ERR_INVALID;
     }
+    if (s->autotune && (!c->tuned[1] || (c->mixed && !c->tuned[0])) && (st = gf_autotune(c, nullptr, nullptr)))
+        return st;
     uint32_t ctr = s->rng_counter;
     // random gauge transformation of every instance (apps/LandauGaugeFixingSU3_4D.cu:192-196)
     if (s->random_trafo) {
@@ -643,6 +689,111 @@ int gf_fix(gf_ctx *c, const gf_schedule *s, gf_report *rep)
             rep[i].chunks = launched;
         }
     }
+    return GF_OK;
+}
+
+// Project-written autotuner: times every candidate launch shape of the OR parity pass on a scratch
+// copy of the context's field (the field itself is not touched; the pass's memory access pattern
+// does not depend on the link values) and keeps the fastest one per precision.
+int gf_autotune(gf_ctx *c, int *choice_fp32, int *choice_fp64)
+{
+    clear_error();
+    int st = check_ctx(c);
+    if (st) return st;
+    static const gf_ctx::PassShape cands[] = {{0, 4, 0}, {1, 2, 0}, {1, 4, 0}, {1, 8, 0}};
+    const int ncand = (int)(sizeof(cands) / sizeof(cands[0]));
+    for (int prec = 0; prec < 2; prec++) {
+        if (prec == 0 && !c->mixed) continue;
+        // scratch field, descriptors and states for this precision
+        const InstDesc &last = c->h_inst.back();
+        const size_t span32 = (size_t)(reinterpret_cast<const char *>(last.f32 ? last.f32 : (float4 *)nullptr) -
+                                       reinterpret_cast<const char *>(c->f32 ? c->f32 : (float4 *)nullptr)) +
+                              (size_t)12 * last.g.V * sizeof(float4);
+        // an instance holds 4 mu x 3 float4 planes (FP32) or 4 mu x 6 double2 planes (FP64) of V
+        const size_t span64 = (size_t)(reinterpret_cast<const char *>(last.f64) - reinterpret_cast<const char *>(c->f64)) +
+                              (size_t)24 * last.g.V * sizeof(double2);
+        const size_t span = prec == 0 ? span32 : span64;
+        void *scratch = nullptr;
+        InstDesc *dinst = nullptr;
+        int *dstate = nullptr;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        auto cleanup = [&]() {
+            cudaFree(scratch);
+            cudaFree(dinst);
+            cudaFree(dstate);
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
+        };
+        if ((st = cuda_status(cudaMalloc(&scratch, span), "autotune scratch"))) {
+            cleanup();
+            return st;
+        }
+        const void *src = prec == 0 ? (const void *)c->f32 : (const void *)c->f64;
+        cudaMemcpyAsync(scratch, src, span, cudaMemcpyDeviceToDevice, c->stream);
+        std::vector<InstDesc> hi = c->h_inst;
+        for (auto &d : hi) {
+            if (prec == 0)
+                d.f32 = reinterpret_cast<float4 *>((char *)scratch + ((char *)d.f32 - (char *)c->f32));
+            else
+                d.f64 = reinterpret_cast<double2 *>((char *)scratch + ((char *)d.f64 - (char *)c->f64));
+        }
+        std::vector<int> hs(c->ninst, prec == 0 ? ST_FP32 : ST_FP64);
+        if ((st = cuda_status(cudaMalloc(&dinst, sizeof(InstDesc) * c->ninst), "cudaMalloc")) ||
+            (st = cuda_status(cudaMalloc(&dstate, sizeof(int) * c->ninst), "cudaMalloc")) ||
+            (st = cuda_status(cudaMemcpyAsync(dinst, hi.data(), sizeof(InstDesc) * c->ninst, cudaMemcpyHostToDevice,
+                                              c->stream), "copy")) ||
+            (st = cuda_status(cudaMemcpyAsync(dstate, hs.data(), sizeof(int) * c->ninst, cudaMemcpyHostToDevice,
+                                              c->stream), "copy")) ||
+            (st = cuda_status(cudaEventCreate(&e0), "event")) || (st = cuda_status(cudaEventCreate(&e1), "event"))) {
+            cleanup();
+            return st;
+        }
+        EngineDev e = c->dev();
+        e.inst = dinst;
+        e.state = dstate;
+        const int want = prec == 0 ? ST_FP32 : ST_FP64;
+        float best = 1e30f;
+        int besti = 0;
+        const long long keep = c->launches;
+        for (int k = 0; k < ncand && !st; k++) {
+            gf_ctx::PassShape sh[2] = {c->shape[0], c->shape[1]};
+            sh[prec] = cands[k];
+            for (int w = 0; w < 2 && !st; w++) st = launch_sweep_on(c, e, sh, ALG_OR, want, 1.7f, 0, 0, 0);
+            cudaEventRecord(e0, c->stream);
+            for (int w = 0; w < 3 && !st; w++) st = launch_sweep_on(c, e, sh, ALG_OR, want, 1.7f, 0, 0, 0);
+            cudaEventRecord(e1, c->stream);
+            if (!st) st = cuda_status(cudaEventSynchronize(e1), "autotune sync");
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (!st && ms < best) {
+                best = ms;
+                besti = k;
+            }
+        }
+        c->launches = keep;
+        cleanup();
+        if (st) return st;
+        c->shape[prec] = cands[besti];
+        c->tuned[prec] = 1;
+    }
+    if (choice_fp32) *choice_fp32 = c->mixed ? (c->shape[0].variant ? c->shape[0].warps : 0) : -1;
+    if (choice_fp64) *choice_fp64 = c->shape[1].variant ? c->shape[1].warps : 0;
+    return GF_OK;
+}
+
+// Set the parity-pass launch shape by hand: variant 0 (one warp per tile) or 1 (pipelined with
+// `warps` = 2, 4 or 8 warps per block).
+int gf_set_pass_shape(gf_ctx *c, int real, int variant, int warps)
+{
+    clear_error();
+    if (!c || !valid_real(real) || (variant != 0 && variant != 1) || (warps != 2 && warps != 4 && warps != 8)) {
+        set_error("invalid pass shape");
+        return GF_ERR_INVALID;
+    }
+    c->shape[real].variant = variant;
+    c->shape[real].warps = warps;
+    c->shape[real].blocks_per_sm = 0;
+    c->tuned[real] = 1;
     return GF_OK;
 }
 

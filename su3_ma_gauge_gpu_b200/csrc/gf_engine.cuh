@@ -78,6 +78,133 @@ __global__ void __launch_bounds__(128) k_batched_pass(EngineDev e, int64_t total
     parity_pass_warp<R, GAUGE, ALGO>(f, f, d.g, warp - d.warp_begin, parity, pi);
 }
 
+// ---- software-pipelined parity pass --------------------------------------------------------------
+// Same site update as k_batched_pass, but every warp walks a strided list of 8-site tiles and
+// prefetches the 2 links of its lane for tile t+1 into shared memory with cp.async (16-byte,
+// L2-only) while it computes tile t.  Each lane reads back only the chunks it copied, so the
+// per-thread cp.async.wait_group is the only synchronisation.  Shared memory per warp:
+// 2 stages x NCH chunks x 32 lanes x 16 B (NCH = 6 for FP32, 12 for FP64).
+template <typename R>
+struct Chunks {
+    static constexpr int per_link = (int)(12 * sizeof(R) / 16);  // 3 (FP32) or 6 (FP64)
+    static constexpr int per_lane = 2 * per_link;
+};
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+struct TileRef {
+    int inst;      // -1: nothing to do
+    int64_t h;     // half-lattice index of this lane's site
+    int64_t s, sd; // up-link site and down-link site
+};
+
+template <typename R>
+__device__ __forceinline__ const uint4 *link_chunks(const InstDesc &d, int64_t s, int mu, int k);
+template <>
+__device__ __forceinline__ const uint4 *link_chunks<float>(const InstDesc &d, int64_t s, int mu, int k)
+{
+    return reinterpret_cast<const uint4 *>(d.f32 + ((int64_t)(mu * 3 + k)) * d.g.V + s);
+}
+template <>
+__device__ __forceinline__ const uint4 *link_chunks<double>(const InstDesc &d, int64_t s, int mu, int k)
+{
+    return reinterpret_cast<const uint4 *>(d.f64 + ((int64_t)(mu * 6 + k)) * d.g.V + s);
+}
+
+template <typename R>
+__device__ __forceinline__ TileRef prefetch_tile(const EngineDev &e, int64_t tile, int parity, int want_state,
+                                                 uint4 *stage)
+{
+    TileRef t{-1, 0, 0, 0};
+    const int i = find_instance(e.inst, e.ninst, tile, [](const InstDesc &d) { return d.warp_begin; });
+    if (e.state[i] != want_state) return t;
+    const InstDesc &d = e.inst[i];
+    const int lane = threadIdx.x & 31, mu = lane >> 3;
+    t.inst = i;
+    t.h = (tile - d.warp_begin) * 8 + (lane & 7);
+    int32_t c[4];
+    site_coords(d.g, t.h, parity, c);
+    t.s = t.h + (parity ? d.g.Vh : 0);
+    t.sd = neighbour_down(d.g, c, mu);
+    constexpr int P = Chunks<R>::per_link;
+#pragma unroll
+    for (int k = 0; k < P; k++) {
+        cp_async16(stage + k * 32 + lane, link_chunks<R>(d, t.s, mu, k));
+        cp_async16(stage + (P + k) * 32 + lane, link_chunks<R>(d, t.sd, mu, k));
+    }
+    return t;
+}
+
+template <typename R>
+__device__ __forceinline__ void unstage_link(const uint4 *stage, int first, Link<R> &L)
+{
+    const int lane = threadIdx.x & 31;
+    R r[12];
+    constexpr int P = Chunks<R>::per_link;
+#pragma unroll
+    for (int k = 0; k < P; k++) {
+        const uint4 v = stage[(first + k) * 32 + lane];
+        const R *pv = reinterpret_cast<const R *>(&v);
+#pragma unroll
+        for (int q = 0; q < (int)(16 / sizeof(R)); q++) r[k * (16 / sizeof(R)) + q] = pv[q];
+    }
+    unpack12(L, r);
+    reconstruct(L);
+}
+
+template <typename R, int GAUGE, int ALGO, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_batched_pass_staged(EngineDev e, int64_t total_warps, int parity,
+                                                                      AlgoParams p, int want_state)
+{
+    extern __shared__ uint4 smem[];
+    constexpr int NCH = Chunks<R>::per_lane;
+    const int w = threadIdx.x >> 5;
+    uint4 *stages[2] = {smem + (2 * w) * NCH * 32, smem + (2 * w + 1) * NCH * 32};
+    const int64_t stride = (int64_t)gridDim.x * WARPS;
+    int64_t tile = (int64_t)blockIdx.x * WARPS + w;
+    int cur = 0;
+    TileRef t = tile < total_warps ? prefetch_tile<R>(e, tile, parity, want_state, stages[0]) : TileRef{-1, 0, 0, 0};
+    cp_async_commit();
+    for (; tile < total_warps; tile += stride) {
+        const int64_t nt = tile + stride;
+        const TileRef n = nt < total_warps ? prefetch_tile<R>(e, nt, parity, want_state, stages[cur ^ 1])
+                                           : TileRef{-1, 0, 0, 0};
+        cp_async_commit();
+        cp_async_wait<1>();
+        if (t.inst >= 0) {
+            const InstDesc &d = e.inst[t.inst];
+            const int mu = (threadIdx.x & 31) >> 3;
+            Link<R> up, dn;
+            unstage_link<R>(stages[cur], 0, up);
+            unstage_link<R>(stages[cur], Chunks<R>::per_link, dn);
+            Rng<R> rng;
+            if (ALGO == ALG_SA || ALGO == ALG_SR || ALGO == ALG_RANDOM)
+                rng.init(ref_rng_tid(t.h), p.seed + (uint32_t)t.inst, p.counter);
+            site_update<GAUGE, ALGO>(up, dn, mu, p, rng);
+            const PackedField<R> f = packed_of<R>(d);
+            store_link<R>(f, t.s, mu, up);
+            store_link<R>(f, t.sd, mu, dn);
+        }
+        __syncwarp();  // every lane is done with stages[cur] before it is refilled
+        t = n;
+        cur ^= 1;
+    }
+    cp_async_wait<0>();
+}
+
+template <typename R>
+constexpr size_t staged_smem_bytes(int warps)
+{
+    return (size_t)warps * 2 * Chunks<R>::per_lane * 32 * 16;
+}
+
 // Quality of every instance in state want_state, with the state transitions of the check:
 //  ST_FP32 -> ST_SWITCH when theta < switch_theta (mixed runs), ST_FP64 -> ST_DONE when
 //  theta < precision; either -> ST_DONE when the sweep budget is spent.  chunk_sweeps is added

@@ -31,7 +31,7 @@ inline double prefactor_a(int) { return 1.0 / 3.0; }
 
 // compile-time dispatch of a functor over the gauge / algorithm template parameters
 template <template <int, int> class K, typename... Args>
-int dispatch_gauge_algo(int gauge, int algo, Args &&...args)
+int dispatch_gauge_algo(int gauge, int algo, const Args &...args)
 {
 #define GFB_CASE_A(G)                                                   \
     switch (algo) {                                                     \

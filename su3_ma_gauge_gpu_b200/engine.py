@@ -41,6 +41,7 @@ class Schedule:
     check_precision: int = 100
     reproject: int = 100
     use_graphs: int = 1
+    autotune: int = 1
 
     def to_c(self) -> _lib.Schedule:
         s = _lib.Schedule()
@@ -126,6 +127,16 @@ class GaugeFixer:
         check(lib().gf_fix(self._h, ctypes.byref(s), reps), "gf_fix")
         return [Report(r.gff, r.theta, r.or_sweeps, r.or_sweeps_fp64, r.sa_sweeps, bool(r.converged), r.chunks)
                 for r in reps]
+
+    def autotune(self):
+        """Time the OR-pass launch shapes and keep the fastest; returns (fp32, fp64) choices."""
+        a, b = ctypes.c_int(), ctypes.c_int()
+        check(lib().gf_autotune(self._h, ctypes.byref(a), ctypes.byref(b)), "gf_autotune")
+        return a.value, b.value
+
+    def set_pass_shape(self, real: str, variant: int, warps: int = 4) -> None:
+        r = _lib.GF_FP64 if real in ("fp64", "double") else _lib.GF_FP32
+        check(lib().gf_set_pass_shape(self._h, r, variant, warps), "gf_set_pass_shape")
 
     def kernel_launches(self) -> int:
         n = ctypes.c_longlong()
