@@ -168,7 +168,9 @@ def run_reference(args):
 
 
 def run_profile_target(nsweeps: int):
-    """A short, fixed launch sequence of the hot kernels for ncu (see profiles/)."""
+    """A short, fixed launch sequence of the hot kernels for ncu (see profiles/): the 32^4 input,
+    `nsweeps` OR sweeps with the direct pass and `nsweeps` with the pipelined pass (4 warps per
+    block), in FP32, then the same in FP64 -- 8 * nsweeps parity-pass launches in this order."""
     import torch
 
     from su3_ma_gauge_gpu_b200 import synthetic as S
@@ -178,14 +180,16 @@ def run_profile_target(nsweeps: int):
     dU = torch.from_numpy(U).cuda()
     with GaugeFixer([SIZE], mixed=True) as gf:
         gf.load(0, dU)
-        gf.sweeps("or", nsweeps, 1.7)
-        gf.to_fp64()
-        gf.sweeps("or", nsweeps, 1.7)
+        for real in ("fp32", "fp64"):
+            if real == "fp64":
+                gf.to_fp64()
+            for variant in (0, 1):
+                gf.set_pass_shape(real, variant, 4)
+                gf.sweeps("or", nsweeps, 1.7)
         g, a = gf.quality()
         gf.store(0, dU)
     torch.cuda.synchronize()
-    print(json.dumps({"profile_target": "ok", "sweeps_per_precision": nsweeps, "F": float(g[0]),
-                      "theta": float(a[0])}))
+    print(json.dumps({"profile_target": "ok", "sweeps_per_shape": nsweeps, "F": float(g[0]), "theta": float(a[0])}))
 
 
 def main():
@@ -290,6 +294,8 @@ def main():
         pass
 
     gf = GaugeFixer([SIZE], mixed=True, stream=stream)
+    gf.load(0, dU_in)
+    tuned = gf.autotune()  # launch shape of the OR pass per precision (0 = direct, else warps/block)
     clocks = ClockSampler(gpu_id)
     ms, rep, launches = timed(gf, step_resident, args.steps, args.warmup)
     clk = clocks.stop()
@@ -355,7 +361,9 @@ def main():
             traffic = None
     roofline = {"bound": "hbm", "achieved": kern[dom]["gbs"], "peak": peak, "unit": "GB/s",
                 "frac": kern[dom]["gbs"] / peak, "traffic": traffic,
-                "kernel": f"k_batched_pass<{'float' if dom == 'fp32' else 'double'}, LANDAU, OR> (one parity pass)",
+                "kernel": (f"k_batched_pass{'_staged' if tuned[0 if dom == 'fp32' else 1] else ''}"
+                           f"<{'float' if dom == 'fp32' else 'double'}, LANDAU, OR> (one parity pass)"),
+                "launch_shape": {"fp32": tuned[0], "fp64": tuned[1]},
                 "algorithmic_bytes_per_launch": Vh * BYTES_PER_SITE_UPDATE[dom], "peak_kind": peak_kind,
                 "per_precision": kern}
 

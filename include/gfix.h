@@ -110,12 +110,18 @@ int gf_stats_destroy(gf_stats *st);
  * The gauge functional and theta always accumulate in FP64.
  * This replaces the per-copy loop of the reference drivers
  * (apps/LandauGaugeFixingSU3_4D.cu:185-283, apps/MAGaugeFixingSU3_4D.cu:197-333), which fix
- * one configuration of compile-time extents at a time.  GF_COULOMB is not accepted here. */
+ * one configuration of compile-time extents at a time.
+ * GF_COULOMB: every lattice is split into its Nt timeslices, which are fixed as independent
+ * instances in the same launches (the reference fixes them one after the other,
+ * apps/CoulombGaugeFixingSU3_4D.cu:199-311).  Their temporal links are not touched while they
+ * sweep: each slice accumulates its gauge transformation W(t,x) instead, and gf_export applies
+ * U_0(t,x) <- W(t,x) U_0(t,x) W(t+1,x)^dagger, which equals the reference's per-sweep left and
+ * right multiplications of U_0 (CoulombKernelsSU3.hxx:226-247). */
 typedef struct gf_ctx gf_ctx;
 
 typedef struct gf_ctx_params {
-    int gauge;             /* GF_LANDAU, GF_MAG or GF_U1XU1 */
-    int ninstances;        /* >= 1 */
+    int gauge;             /* GF_LANDAU, GF_COULOMB, GF_MAG or GF_U1XU1 */
+    int ninstances;        /* number of lattices, >= 1 */
     const int32_t *sizes;  /* 4 * ninstances extents {Nt, Nx, Ny, Nz}, all even */
     int mixed;             /* 1: FP32 bulk + FP64 polish, 0: FP64 only */
     void *stream;          /* cudaStream_t to run on, or NULL for a stream of the context's own */
@@ -130,7 +136,7 @@ typedef struct gf_schedule {
     int sa_steps;          /* sasteps */
     float sa_min, sa_max;  /* samin, samax */
     int sa_geometric;      /* 0: linear temperature steps (reference), 1: geometric */
-    int micro_updates;     /* microupdates after each SA sweep */
+    int micro_updates;     /* microupdates after each (micro_every-th) SA sweep */
     int or_max_iter;       /* ormaxiter: OR sweep budget (FP32 + FP64) */
     float or_parameter;    /* orparameter (omega) */
     double precision;      /* stop when theta < precision */
@@ -139,6 +145,7 @@ typedef struct gf_schedule {
     int reproject;         /* reproject: sweeps between reunitarisations */
     int use_graphs;        /* 1: replay check chunks from CUDA graphs */
     int autotune;          /* 1: gf_autotune first if the context is not tuned yet */
+    int micro_every;       /* micro steps after every micro_every-th SA sweep (reference: 1) */
 } gf_schedule;
 
 typedef struct gf_report {
@@ -152,22 +159,26 @@ typedef struct gf_report {
 
 int gf_create(const gf_ctx_params *params, gf_ctx **out);
 int gf_destroy(gf_ctx *ctx);
-/* Load instance `instance` from a GpuPattern array (float or double; device memory, or host
- * memory with on_host = 1, in which case only rows 0,1 are copied).  Resets its state. */
-int gf_import(gf_ctx *ctx, int instance, int real, const void *U, int on_host);
-/* Write instance `instance` back as a GpuPattern array, reunitarised in FP64 with row 2
- * rebuilt (the reference's closing projectSU3, apps/LandauGaugeFixingSU3_4D.cu:271). */
-int gf_export(gf_ctx *ctx, int instance, int real, void *U, int on_host);
+/* Load lattice `lattice` (0 .. ninstances-1) from a GpuPattern array (float or double; device
+ * memory, or host memory with on_host = 1, in which case only rows 0,1 are copied); for
+ * GF_COULOMB the array holds its Nt timeslices one after the other (GpuPatternTimeslice,
+ * access_pattern/GpuPatternTimeslice.hxx:57-62).  Resets the state of its instances. */
+int gf_import(gf_ctx *ctx, int lattice, int real, const void *U, int on_host);
+/* Write lattice `lattice` back in the same layout, reunitarised in FP64 with row 2 rebuilt
+ * (the reference's closing projectSU3, apps/LandauGaugeFixingSU3_4D.cu:271). */
+int gf_export(gf_ctx *ctx, int lattice, int real, void *U, int on_host);
 /* nsweeps full sweeps (both parities) of one algorithm (0 OR, 1 micro, 2 SA, 3 SR, 4 random
  * trafo) on every instance still sweeping; Philox counters rng_counter, rng_counter+1, ... */
 int gf_sweeps(gf_ctx *ctx, int algo, int nsweeps, float param, int seed, int rng_counter);
-/* FP64 functional and theta of every instance (arrays of ninstances doubles). */
+/* FP64 functional and theta of every instance (one per lattice, or per timeslice for
+ * GF_COULOMB: arrays of that many doubles). */
 int gf_quality_all(gf_ctx *ctx, double *gff, double *theta);
 /* Reunitarise every instance in its current storage (FP64 arithmetic). */
 int gf_reunitarize(gf_ctx *ctx);
 /* Move every FP32 instance of a mixed context to FP64 storage (reunitarised in FP64). */
 int gf_set_storage(gf_ctx *ctx, int real);
-/* The whole per-copy schedule for all instances; reports has ninstances entries (or NULL). */
+/* The whole per-copy schedule for all instances; reports has one entry per instance (per
+ * timeslice for GF_COULOMB), or NULL. */
 int gf_fix(gf_ctx *ctx, const gf_schedule *schedule, gf_report *reports);
 /* Autotuner: times the candidate launch shapes of the OR parity pass (one warp per 8-site tile;
  * pipelined with cp.async prefetch and 2, 4 or 8 warps per block) on a scratch copy of the
@@ -176,6 +187,8 @@ int gf_fix(gf_ctx *ctx, const gf_schedule *schedule, gf_report *reports);
 int gf_autotune(gf_ctx *ctx, int *choice_fp32, int *choice_fp64);
 /* Fix the launch shape instead: variant 0 (direct) or 1 (pipelined, warps = 2, 4 or 8). */
 int gf_set_pass_shape(gf_ctx *ctx, int real, int variant, int warps);
+/* Number of instances (lattices, or timeslices for GF_COULOMB). */
+int gf_instances(gf_ctx *ctx);
 /* Number of kernels this context has launched so far (each node of a replayed graph counts). */
 int gf_kernel_launches(gf_ctx *ctx, long long *count);
 

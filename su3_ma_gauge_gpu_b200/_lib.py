@@ -65,7 +65,7 @@ class Schedule(ctypes.Structure):
                 ("sa_geometric", ctypes.c_int), ("micro_updates", ctypes.c_int), ("or_max_iter", ctypes.c_int),
                 ("or_parameter", ctypes.c_float), ("precision", ctypes.c_double), ("switch_theta", ctypes.c_double),
                 ("check_precision", ctypes.c_int), ("reproject", ctypes.c_int), ("use_graphs", ctypes.c_int),
-                ("autotune", ctypes.c_int)]
+                ("autotune", ctypes.c_int), ("micro_every", ctypes.c_int)]
 
 
 class Report(ctypes.Structure):
@@ -89,6 +89,7 @@ SIGNATURES.update({
     "gf_kernel_launches": (_c_int, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
     "gf_autotune": (_c_int, [_vp, ctypes.POINTER(_c_int), ctypes.POINTER(_c_int)]),
     "gf_set_pass_shape": (_c_int, [_vp, _c_int, _c_int, _c_int]),
+    "gf_instances": (_c_int, [_vp]),
 })
 
 _LIB = None

@@ -11,6 +11,7 @@
 //  - the OR loop is captured as a CUDA graph of one check chunk and replayed; the host only
 //    reads the per-instance states (pinned memory) one chunk behind.
 #include <algorithm>
+#include <array>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -47,6 +48,14 @@ struct gf_ctx {
         int variant = 0, warps = 4, blocks_per_sm = 0;
     } shape[2];
     int tuned[2] = {0, 0};
+    // the lattices the caller passed: first instance and number of instances (Coulomb contexts
+    // split every lattice into its Nt timeslices; the other gauges have one instance each)
+    struct Lattice {
+        int first, count;
+        int64_t slice_reals;  // reals of one instance's GpuPattern array (V * 72)
+    };
+    std::vector<Lattice> lattices;
+    double2 *t64 = nullptr;   // Coulomb: original temporal links of every timeslice
 
     EngineDev dev() const
     {
@@ -83,6 +92,13 @@ int launch_staged(const gf_ctx *c, const EngineDev &e, const PassArgs &a, int bl
 {
     const size_t smem = staged_smem_bytes<R>(WARPS);
     auto kern = k_batched_pass_staged<R, GAUGE, ALGO, WARPS>;
+    static bool smem_opt_in = false;  // above 48 KB the dynamic shared memory must be opted in
+    if (!smem_opt_in) {
+        int st = cuda_status(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                             "cudaFuncSetAttribute");
+        if (st) return st;
+        smem_opt_in = true;
+    }
     int occ = blocks_per_sm;
     if (occ <= 0) {
         int o = 0;
@@ -242,10 +258,6 @@ int gf_create(const gf_ctx_params *p, gf_ctx **out)
         set_error("invalid gf_ctx_params");
         return GF_ERR_INVALID;
     }
-    if (p->gauge == GF_COULOMB) {
-        set_error("GF_COULOMB contexts are not supported by the batched engine; use the plugin entry points");
-        return GF_ERR_UNSUPPORTED;
-    }
     *out = nullptr;
     gf_ctx *c = new (std::nothrow) gf_ctx();
     if (!c) {
@@ -253,15 +265,39 @@ int gf_create(const gf_ctx_params *p, gf_ctx **out)
         return GF_ERR_NOMEM;
     }
     c->gauge = p->gauge;
-    c->ninst = p->ninstances;
     c->mixed = p->mixed ? 1 : 0;
     cudaGetDevice(&c->device);
     cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device);
+    const bool coulomb = p->gauge == GF_COULOMB;
+    // expand the lattices into instances (Coulomb: one per timeslice, geometry {1, Nx, Ny, Nz})
+    std::vector<std::array<int32_t, 4>> inst_sizes;
+    std::vector<int> inst_next;
+    for (int l = 0; l < p->ninstances; l++) {
+        const int32_t *sz = p->sizes + 4 * l;
+        const int nt = coulomb ? sz[0] : 1;
+        if (coulomb && (nt < 2 || (nt & 1))) {
+            set_error("Coulomb lattice %d: Nt = %d must be even and >= 2", l, nt);
+            delete c;
+            return GF_ERR_INVALID;
+        }
+        const int first = (int)inst_sizes.size();
+        const int64_t vol = coulomb ? (int64_t)sz[1] * sz[2] * sz[3] : (int64_t)sz[0] * sz[1] * sz[2] * sz[3];
+        c->lattices.push_back({first, nt, vol * 72});
+        for (int t = 0; t < nt; t++) {
+            inst_sizes.push_back(coulomb ? std::array<int32_t, 4>{1, sz[1], sz[2], sz[3]}
+                                         : std::array<int32_t, 4>{sz[0], sz[1], sz[2], sz[3]});
+            inst_next.push_back(coulomb ? first + (t + 1) % nt : -1);
+        }
+    }
+    c->ninst = (int)inst_sizes.size();
     int st = GF_OK;
-    int64_t voff = 0, woff = 0, loff = 0, qoff = 0;
+    int64_t voff = 0, woff = 0, loff = 0, qoff = 0, toff = 0;
     for (int i = 0; i < c->ninst && !st; i++) {
         InstDesc d{};
-        st = make_geom(p->sizes + 4 * i, p->gauge, false, d.g);
+        st = make_geom(inst_sizes[i].data(), p->gauge, coulomb, d.g);
+        d.next = inst_next[i];
+        d.t64 = coulomb ? reinterpret_cast<double2 *>(toff) : nullptr;  // rebased after allocation
+        toff += 6 * d.g.V;
         d.warp_begin = woff;
         d.link_begin = loff;
         d.qblock_begin = qoff;
@@ -300,10 +336,13 @@ int gf_create(const gf_ctx_params *p, gf_ctx **out)
     if (c->mixed && (st = cuda_status(cudaMalloc(&c->f32, n32 * sizeof(float4)), "cudaMalloc FP32 field")))
         return fail(st);
     if ((st = cuda_status(cudaMalloc(&c->f64, n64 * sizeof(double2)), "cudaMalloc FP64 field"))) return fail(st);
+    if (coulomb && (st = cuda_status(cudaMalloc(&c->t64, (size_t)toff * sizeof(double2)), "cudaMalloc temporal links")))
+        return fail(st);
     for (auto &d : c->h_inst) {
         const size_t off = (size_t)reinterpret_cast<uintptr_t>(d.f32);
         d.f32 = c->mixed ? c->f32 + off : nullptr;
         d.f64 = c->f64 + 2 * off;
+        if (coulomb) d.t64 = c->t64 + (size_t)reinterpret_cast<uintptr_t>(d.t64);
     }
     const int n = c->ninst;
     if ((st = cuda_status(cudaMalloc(&c->d_inst, sizeof(InstDesc) * n), "cudaMalloc"))) return fail(st);
@@ -348,6 +387,7 @@ int gf_destroy(gf_ctx *c)
     if (c->stream) cudaStreamSynchronize(c->stream);
     cudaFree(c->f32);
     cudaFree(c->f64);
+    cudaFree(c->t64);
     cudaFree(c->d_inst);
     cudaFree(c->d_state);
     cudaFree(c->d_quality);
@@ -375,94 +415,103 @@ static int ensure_staging(gf_ctx *c, size_t bytes)
     return st;
 }
 
-int gf_import(gf_ctx *c, int instance, int real, const void *U, int on_host)
+// Import lattice `lat` (GpuPattern; for Coulomb the GpuPatternTimeslice array of Nt slices,
+// apps/CoulombGaugeFixingSU3_4D.cu:57-59,132-134) into its instances and reset their state.
+int gf_import(gf_ctx *c, int lat, int real, const void *U, int on_host)
 {
     clear_error();
     int st = check_ctx(c);
     if (st) return st;
-    if (instance < 0 || instance >= c->ninst || !U || !valid_real(real)) {
-        set_error("invalid instance, field or real type");
+    if (lat < 0 || lat >= (int)c->lattices.size() || !U || !valid_real(real)) {
+        set_error("invalid lattice index, field or real type");
         return GF_ERR_INVALID;
     }
-    const InstDesc &d = c->h_inst[instance];
+    const gf_ctx::Lattice &L = c->lattices[lat];
     const size_t es = real == GF_FP64 ? 8 : 4;
-    const void *src = U;
+    const char *src = (const char *)U;
     if (on_host) {
         // only the 12 planes of rows 0,1 of every mu travel (GpuPattern keeps them contiguous)
-        if ((st = ensure_staging(c, (size_t)d.g.V * 72 * es))) return st;
-        for (int mu = 0; mu < 4; mu++) {
-            const size_t off = (size_t)mu * 18 * d.g.V * es;
-            if ((st = cuda_status(cudaMemcpyAsync((char *)c->staging + off, (const char *)U + off, 12 * d.g.V * es,
-                                                  cudaMemcpyHostToDevice, c->stream), "H2D")))
-                return st;
+        if ((st = ensure_staging(c, (size_t)L.slice_reals * L.count * es))) return st;
+        for (int t = 0; t < L.count; t++) {
+            const int64_t V = c->h_inst[L.first + t].g.V;
+            for (int mu = 0; mu < 4; mu++) {
+                const size_t off = ((size_t)t * L.slice_reals + (size_t)mu * 18 * V) * es;
+                if ((st = cuda_status(cudaMemcpyAsync((char *)c->staging + off, (const char *)U + off, 12 * V * es,
+                                                      cudaMemcpyHostToDevice, c->stream), "H2D")))
+                    return st;
+            }
         }
-        src = c->staging;
+        src = (const char *)c->staging;
     }
-    const unsigned blocks = grid_for(4 * d.g.V, 256);
     const int target = c->mixed ? ST_FP32 : ST_FP64;
-    if (target == ST_FP32) {
-        if (real == GF_FP64) k_import<double, float><<<blocks, 256, 0, c->stream>>>(c->dev(), instance, (const double *)src);
-        else k_import<float, float><<<blocks, 256, 0, c->stream>>>(c->dev(), instance, (const float *)src);
-    } else {
-        if (real == GF_FP64) k_import<double, double><<<blocks, 256, 0, c->stream>>>(c->dev(), instance, (const double *)src);
-        else k_import<float, double><<<blocks, 256, 0, c->stream>>>(c->dev(), instance, (const float *)src);
+    for (int t = 0; t < L.count; t++) {
+        const int i = L.first + t;
+        const InstDesc &d = c->h_inst[i];
+        const unsigned blocks = grid_for(4 * d.g.V, 256);
+        const void *sp = src + (size_t)t * L.slice_reals * es;
+        if (target == ST_FP32) {
+            if (real == GF_FP64) k_import<double, float><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (const double *)sp);
+            else k_import<float, float><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (const float *)sp);
+        } else {
+            if (real == GF_FP64) k_import<double, double><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (const double *)sp);
+            else k_import<float, double><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (const float *)sp);
+        }
+        c->launches++;
+        if ((st = launch_status("import"))) return st;
     }
-    c->launches++;
-    if ((st = launch_status("import"))) return st;
-    const int z[2] = {0, 0};
-    const int stor = target == ST_FP32 ? 0 : 1;
-    if ((st = cuda_status(cudaMemcpyAsync(c->d_state + instance, &target, sizeof(int), cudaMemcpyHostToDevice,
-                                          c->stream), "state")))
-        return st;
-    if ((st = cuda_status(cudaMemcpyAsync(c->d_storage + instance, &stor, sizeof(int), cudaMemcpyHostToDevice,
-                                          c->stream), "storage")))
-        return st;
-    if ((st = cuda_status(cudaMemcpyAsync(c->d_sweeps + instance, z, sizeof(int), cudaMemcpyHostToDevice, c->stream),
-                          "sweeps")))
-        return st;
-    if ((st = cuda_status(cudaMemcpyAsync(c->d_sweeps64 + instance, z, sizeof(int), cudaMemcpyHostToDevice,
-                                          c->stream), "sweeps")))
+    const int n = L.count;
+    std::vector<int> states(n, target), stor(n, target == ST_FP32 ? 0 : 1), zeros(n, 0);
+    if ((st = cuda_status(cudaMemcpyAsync(c->d_state + L.first, states.data(), sizeof(int) * n,
+                                          cudaMemcpyHostToDevice, c->stream), "state")) ||
+        (st = cuda_status(cudaMemcpyAsync(c->d_storage + L.first, stor.data(), sizeof(int) * n,
+                                          cudaMemcpyHostToDevice, c->stream), "storage")) ||
+        (st = cuda_status(cudaMemcpyAsync(c->d_sweeps + L.first, zeros.data(), sizeof(int) * n,
+                                          cudaMemcpyHostToDevice, c->stream), "sweeps")) ||
+        (st = cuda_status(cudaMemcpyAsync(c->d_sweeps64 + L.first, zeros.data(), sizeof(int) * n,
+                                          cudaMemcpyHostToDevice, c->stream), "sweeps")))
         return st;
     return cuda_status(cudaStreamSynchronize(c->stream), "import sync");
 }
 
-// which field currently holds the instance
-static int storage_of(gf_ctx *c, int instance, int &st)
-{
-    st = sync_states(c);
-    return c->h_state[c->ninst + instance] == 0 ? GF_FP32 : GF_FP64;
-}
-
-int gf_export(gf_ctx *c, int instance, int real, void *U, int on_host)
+// Export lattice `lat`, reunitarised in FP64 with row 2 rebuilt; Coulomb lattices get their
+// temporal links transformed by the accumulated W of slices t and t+1.
+int gf_export(gf_ctx *c, int lat, int real, void *U, int on_host)
 {
     clear_error();
     int st = check_ctx(c);
     if (st) return st;
-    if (instance < 0 || instance >= c->ninst || !U || !valid_real(real)) {
-        set_error("invalid instance, field or real type");
+    if (lat < 0 || lat >= (int)c->lattices.size() || !U || !valid_real(real)) {
+        set_error("invalid lattice index, field or real type");
         return GF_ERR_INVALID;
     }
-    const InstDesc &d = c->h_inst[instance];
+    const gf_ctx::Lattice &L = c->lattices[lat];
     const size_t es = real == GF_FP64 ? 8 : 4;
-    const int stor = storage_of(c, instance, st);
-    if (st) return st;
-    void *dst = U;
+    if ((st = sync_states(c))) return st;
+    char *dst = (char *)U;
     if (on_host) {
-        if ((st = ensure_staging(c, (size_t)d.g.V * 72 * es))) return st;
-        dst = c->staging;
+        if ((st = ensure_staging(c, (size_t)L.slice_reals * L.count * es))) return st;
+        dst = (char *)c->staging;
     }
-    const unsigned blocks = grid_for(4 * d.g.V, 256);
-    if (stor == GF_FP32) {
-        if (real == GF_FP64) k_export<float, double><<<blocks, 256, 0, c->stream>>>(c->dev(), instance, (double *)dst);
-        else k_export<float, float><<<blocks, 256, 0, c->stream>>>(c->dev(), instance, (float *)dst);
-    } else {
-        if (real == GF_FP64) k_export<double, double><<<blocks, 256, 0, c->stream>>>(c->dev(), instance, (double *)dst);
-        else k_export<double, float><<<blocks, 256, 0, c->stream>>>(c->dev(), instance, (float *)dst);
+    for (int t = 0; t < L.count; t++) {
+        const int i = L.first + t;
+        const InstDesc &d = c->h_inst[i];
+        const unsigned blocks = grid_for(4 * d.g.V, 256);
+        void *dp = dst + (size_t)t * L.slice_reals * es;
+        if (c->gauge == GF_COULOMB) {
+            if (real == GF_FP64) k_export_coulomb<double><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (double *)dp);
+            else k_export_coulomb<float><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (float *)dp);
+        } else if (c->h_state[c->ninst + i] == 0) {
+            if (real == GF_FP64) k_export<float, double><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (double *)dp);
+            else k_export<float, float><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (float *)dp);
+        } else {
+            if (real == GF_FP64) k_export<double, double><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (double *)dp);
+            else k_export<double, float><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (float *)dp);
+        }
+        c->launches++;
+        if ((st = launch_status("export"))) return st;
     }
-    c->launches++;
-    if ((st = launch_status("export"))) return st;
-    if (on_host &&
-        (st = cuda_status(cudaMemcpyAsync(U, dst, (size_t)d.g.V * 72 * es, cudaMemcpyDeviceToHost, c->stream), "D2H")))
+    if (on_host && (st = cuda_status(cudaMemcpyAsync(U, dst, (size_t)L.slice_reals * L.count * es,
+                                                     cudaMemcpyDeviceToHost, c->stream), "D2H")))
         return st;
     return cuda_status(cudaStreamSynchronize(c->stream), "export sync");
 }
@@ -572,7 +621,10 @@ int gf_fix(gf_ctx *c, const gf_schedule *s, gf_report *rep)
             const float Ti = s->sa_geometric ? (float)(s->sa_max * pow(ratio, (double)i)) : T;
             if ((st = gf_sweeps(c, ALG_SA, 1, Ti, (int)s->seed, (int)ctr))) return st;
             ctr += 2;
-            if (s->micro_updates > 0 && (st = gf_sweeps(c, ALG_MICRO, s->micro_updates, 0.f, 0, 0))) return st;
+            const int every = s->micro_every > 0 ? s->micro_every : 1;
+            if (s->micro_updates > 0 && (i % every) == every - 1 &&
+                (st = gf_sweeps(c, ALG_MICRO, s->micro_updates, 0.f, 0, 0)))
+                return st;
             if (i % s->reproject == 0 && (st = gf_reunitarize(c))) return st;
             T -= dT;
         }
@@ -701,7 +753,8 @@ int gf_autotune(gf_ctx *c, int *choice_fp32, int *choice_fp64)
     int st = check_ctx(c);
     if (st) return st;
     static const gf_ctx::PassShape cands[] = {{0, 4, 0}, {1, 2, 0}, {1, 4, 0}, {1, 8, 0}};
-    const int ncand = (int)(sizeof(cands) / sizeof(cands[0]));
+    // the pipelined pass does not implement the Coulomb W tracking: direct pass only
+    const int ncand = c->gauge == GF_COULOMB ? 1 : (int)(sizeof(cands) / sizeof(cands[0]));
     for (int prec = 0; prec < 2; prec++) {
         if (prec == 0 && !c->mixed) continue;
         // scratch field, descriptors and states for this precision
@@ -786,8 +839,9 @@ int gf_autotune(gf_ctx *c, int *choice_fp32, int *choice_fp64)
 int gf_set_pass_shape(gf_ctx *c, int real, int variant, int warps)
 {
     clear_error();
-    if (!c || !valid_real(real) || (variant != 0 && variant != 1) || (warps != 2 && warps != 4 && warps != 8)) {
-        set_error("invalid pass shape");
+    if (!c || !valid_real(real) || (variant != 0 && variant != 1) || (warps != 2 && warps != 4 && warps != 8) ||
+        (variant == 1 && c->gauge == GF_COULOMB)) {
+        set_error("invalid pass shape (Coulomb contexts use the direct pass)");
         return GF_ERR_INVALID;
     }
     c->shape[real].variant = variant;
@@ -796,6 +850,8 @@ int gf_set_pass_shape(gf_ctx *c, int real, int variant, int warps)
     c->tuned[real] = 1;
     return GF_OK;
 }
+
+int gf_instances(gf_ctx *c) { return c ? c->ninst : 0; }
 
 int gf_kernel_launches(gf_ctx *c, long long *count)
 {

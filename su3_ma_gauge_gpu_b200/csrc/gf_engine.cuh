@@ -24,6 +24,8 @@ struct InstDesc {
     int64_t qblocks;      // quality blocks of this instance
     float4 *f32;          // packed FP32 field (may be null in plain-FP64 contexts)
     double2 *f64;         // packed FP64 field
+    double2 *t64;         // Coulomb: the slice's original temporal links (6 double2 planes), else null
+    int next;             // Coulomb: instance of timeslice t+1 of the same lattice, else -1
 };
 
 struct EngineDev {
@@ -75,7 +77,7 @@ __global__ void __launch_bounds__(128) k_batched_pass(EngineDev e, int64_t total
     const PackedField<R> f = packed_of<R>(d);
     AlgoParams pi = p;
     pi.seed = p.seed + (uint32_t)i;
-    parity_pass_warp<R, GAUGE, ALGO>(f, f, d.g, warp - d.warp_begin, parity, pi);
+    parity_pass_warp<R, GAUGE, ALGO, PackedField<R>, GAUGE == COULOMB>(f, f, d.g, warp - d.warp_begin, parity, pi);
 }
 
 // ---- software-pipelined parity pass --------------------------------------------------------------
@@ -287,6 +289,15 @@ __global__ void __launch_bounds__(256) k_import(EngineDev e, int i, const Rin *U
     R o[12];
 #pragma unroll
     for (int k = 0; k < 12; k++) o[k] = (R)r[k];
+    if (d.t64 && mu == 0) {
+        // Coulomb: keep the temporal link in FP64 and start W at the identity
+        double t[12];
+#pragma unroll
+        for (int k = 0; k < 12; k++) t[k] = (double)r[k];
+        PackedField<double>{d.t64, d.g.V}.store12(s, 0, t);
+#pragma unroll
+        for (int k = 0; k < 12; k++) o[k] = (k == 0 || k == 8) ? (R)1 : (R)0;  // rows 0,1 of 1
+    }
     packed_of<R>(d).store12(s, mu, o);
 }
 
@@ -302,6 +313,67 @@ __global__ void __launch_bounds__(256) k_export(EngineDev e, int i, Rout *U)
     const int64_t s = idx - mu * d.g.V;
     Link<double> L;
     load_link_f64<R>(packed_of<R>(d), s, mu, L);
+    project_rows(L);
+    Link<Rout> o;
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) o.e[a][b] = cx<Rout>((Rout)L.e[a][b].x, (Rout)L.e[a][b].y);
+    RefField<Rout>{U, d.g.V}.store18(s, mu, o);
+}
+
+// Coulomb export of timeslice i: spatial links as k_export; temporal links
+// U_0(t,x) <- W(t,x) U_0(t,x) W(t+1,x)^dagger, W read from each slice's current storage.
+template <typename Rout>
+__global__ void __launch_bounds__(256) k_export_coulomb(EngineDev e, int i, Rout *U)
+{
+    const InstDesc d = e.inst[i];
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= 4 * d.g.V) return;
+    const int mu = (int)(idx / d.g.V);
+    const int64_t s = idx - mu * d.g.V;
+    Link<double> L;
+    const bool own64 = e.storage[i] == 1;
+    if (mu != 0) {
+        if (own64) load_link_f64<double>(packed_of<double>(d), s, mu, L);
+        else load_link_f64<float>(packed_of<float>(d), s, mu, L);
+    } else {
+        const InstDesc dn = e.inst[d.next];
+        Link<double> W, Wn, T;
+        if (own64) load_link_f64<double>(packed_of<double>(d), s, 0, W);
+        else load_link_f64<float>(packed_of<float>(d), s, 0, W);
+        if (e.storage[d.next] == 1) load_link_f64<double>(packed_of<double>(dn), s, 0, Wn);
+        else load_link_f64<float>(packed_of<float>(dn), s, 0, Wn);
+        load_link_f64<double>(PackedField<double>{d.t64, d.g.V}, s, 0, T);
+        Link<double> M;  // W T
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+#pragma unroll
+            for (int b = 0; b < 3; b++) {
+                Cx<double> acc = cx<double>(0, 0);
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    const Cx<double> t = cmul(W.e[a][k], T.e[k][b]);
+                    acc.x += t.x;
+                    acc.y += t.y;
+                }
+                M.e[a][b] = acc;
+            }
+#pragma unroll
+        for (int a = 0; a < 2; a++)  // rows 0,1 of M Wn^dagger; row 2 is rebuilt by project_rows
+#pragma unroll
+            for (int b = 0; b < 3; b++) {
+                Cx<double> acc = cx<double>(0, 0);
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    const Cx<double> w = Wn.e[b][k];
+                    const Cx<double> t = cmul(M.e[a][k], cx<double>(w.x, -w.y));
+                    acc.x += t.x;
+                    acc.y += t.y;
+                }
+                L.e[a][b] = acc;
+            }
+    }
     project_rows(L);
     Link<Rout> o;
 #pragma unroll

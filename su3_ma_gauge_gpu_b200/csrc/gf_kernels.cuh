@@ -16,7 +16,13 @@ __host__ __device__ constexpr double prefactor_gff_dev(int gauge) { return gauge
 // even extents, so a warp is either fully inside the parity half or fully outside.
 // Fup holds the up links and every down link except, for COULOMB, the temporal down link, which
 // comes from the slice t-1 field Fdw at the same spatial site (CoulombKernelsSU3.hxx:226-234).
-template <typename R, int GAUGE, int ALGO, class F>
+// TRACK_W (batched Coulomb): the mu = 0 planes of a timeslice hold W(x), the gauge transformation
+// accumulated at that site, instead of temporal links.  Lane mu = 0 left-multiplies W by every g
+// (W <- g W) and has no down link; the temporal links themselves are transformed once, at the end,
+// as U_0(t,x) <- W(t,x) U_0(t,x) W(t+1,x)^dagger (the product of the reference's per-sweep left and
+// right multiplications, CoulombKernelsSU3.hxx:226-247), so timeslices share no memory while they
+// sweep.
+template <typename R, int GAUGE, int ALGO, class F, bool TRACK_W = false>
 __device__ __forceinline__ void parity_pass_warp(const F &Fup, const F &Fdw, const Geom &g, int64_t warp, int parity,
                                                  const AlgoParams &p)
 {
@@ -27,17 +33,25 @@ __device__ __forceinline__ void parity_pass_warp(const F &Fup, const F &Fdw, con
     site_coords(g, h, parity, c);
     const int64_t s = h + (parity ? g.Vh : 0);
     const bool tdown = (GAUGE == COULOMB) && (mu == 0);
+    const bool wlane = TRACK_W && tdown;
     const int64_t sd = tdown ? s : neighbour_down(g, c, mu);
     Link<R> up, dn;
     load_link<R>(Fup, s, mu, up);
-    if (tdown)
+    if (wlane) {
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) dn.e[i][j] = cx<R>(i == j ? (R)1 : (R)0, (R)0);
+    } else if (tdown) {
         load_link<R>(Fdw, sd, mu, dn);
-    else
+    } else {
         load_link<R>(Fup, sd, mu, dn);
+    }
     Rng<R> rng;
     if (ALGO == ALG_SA || ALGO == ALG_SR || ALGO == ALG_RANDOM) rng.init(ref_rng_tid(h), p.seed, p.counter);
     site_update<GAUGE, ALGO>(up, dn, mu, p, rng);
     store_link<R>(Fup, s, mu, up);
+    if (wlane) return;
     if (tdown)
         store_link<R>(Fdw, sd, mu, dn);
     else

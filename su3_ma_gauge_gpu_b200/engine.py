@@ -18,7 +18,7 @@ from . import _lib
 from ._lib import check, lib
 
 ALGOS = {"or": 0, "micro": 1, "sa": 2, "sr": 3, "random": 4}
-GAUGES = {"landau": _lib.GF_LANDAU, "mag": _lib.GF_MAG, "u1xu1": _lib.GF_U1XU1}
+GAUGES = {"landau": _lib.GF_LANDAU, "coulomb": _lib.GF_COULOMB, "mag": _lib.GF_MAG, "u1xu1": _lib.GF_U1XU1}
 
 
 @dataclass
@@ -42,6 +42,7 @@ class Schedule:
     reproject: int = 100
     use_graphs: int = 1
     autotune: int = 1
+    micro_every: int = 1
 
     def to_c(self) -> _lib.Schedule:
         s = _lib.Schedule()
@@ -71,7 +72,11 @@ def _real(a) -> int:
 
 
 class GaugeFixer:
-    """A gf_ctx: ``sizes`` is a list of (Nt, Nx, Ny, Nz), one per instance."""
+    """A gf_ctx: ``sizes`` is a list of lattices (Nt, Nx, Ny, Nz).
+
+    For gauge="coulomb" every lattice is fixed as Nt independent timeslices (instances);
+    load/store take the lattice index and the GpuPatternTimeslice array of all its slices,
+    reports and quality() are per timeslice."""
 
     def __init__(self, sizes, gauge="landau", mixed=True, stream=None):
         self.sizes = [tuple(int(v) for v in s) for s in sizes]
@@ -87,7 +92,7 @@ class GaugeFixer:
 
     @property
     def ninstances(self) -> int:
-        return len(self.sizes)
+        return lib().gf_instances(self._h)
 
     def load(self, i: int, U) -> None:
         """Import instance i from a GpuPattern array: CUDA tensor, or numpy array (host)."""

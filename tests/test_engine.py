@@ -208,3 +208,81 @@ def test_autotune_picks_a_shape(cuda):
         after = np.zeros_like(U)
         gf.store(0, after)
         assert np.array_equal(before, after)  # tuning ran on a scratch copy
+
+
+def _coulomb_reference_flow(torch, U, size, nsweeps, algo="or", param=1.7, seed=0, counter=0):
+    """The reference's Coulomb app flow through the plugin ABI: timeslices one after the other,
+    each with UtUp = slice t and UtDw = slice t-1 (apps/CoulombGaugeFixingSU3_4D.cu:199-311)."""
+    import ctypes
+
+    from su3_ma_gauge_gpu_b200 import _lib
+
+    L = _lib.lib()
+    Nt = size[0]
+    Vs = int(np.prod(size[1:]))
+    slices = [torch.from_numpy(U[t * Vs * 72:(t + 1) * Vs * 72].copy()).cuda() for t in range(Nt)]
+    ss = _lib.size_arg((1,) + tuple(size[1:]))
+    for t in range(Nt):
+        up, dw = slices[t], slices[(t - 1) % Nt]
+        for k in range(nsweeps):
+            for parity in (0, 1):
+                if algo == "or":
+                    st = L.gf_or_step(1, 1, up.data_ptr(), dw.data_ptr(), ss, parity, ctypes.c_float(param), None)
+                else:
+                    st = L.gf_sa_step(1, 1, up.data_ptr(), dw.data_ptr(), ss, parity, ctypes.c_float(param),
+                                      seed + t, counter + 2 * k + parity, None)
+                _lib.check(st, "coulomb step")
+    for t in range(Nt):
+        _lib.check(L.gf_project_su3(1, slices[t].data_ptr(), ss, None), "project")
+    return np.concatenate([s.cpu().numpy() for s in slices])
+
+
+@pytest.mark.parametrize("algo", ["or", "sa"])
+def test_coulomb_batched_matches_sequential_timeslices(cuda, algo):
+    """All timeslices in one launch (W tracking) == the reference's slice-by-slice loop."""
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer
+
+    torch = cuda
+    size = (4, 4, 6, 4)
+    Vs = int(np.prod(size[1:]))
+    # the reference's timeslice layout: Nt consecutive GpuPattern arrays of {1, Nx, Ny, Nz}
+    U = np.concatenate([S.smooth_config((1,) + size[1:], 0.3, 60 + t)[0] for t in range(size[0])])
+    n = 3
+    param = 1.7 if algo == "or" else 0.6
+    ref = _coulomb_reference_flow(torch, U, size, n, algo, param, seed=7, counter=5)
+    with GaugeFixer([size], gauge="coulomb", mixed=False) as gf:
+        assert gf.ninstances == size[0]
+        gf.load(0, U)
+        gf.sweeps(algo, n, param, seed=7, rng_counter=5)
+        out = np.zeros_like(U)
+        gf.store(0, out)
+    a = out.reshape(size[0], 4, 3, 3, 2, Vs)
+    b = ref.reshape(size[0], 4, 3, 3, 2, Vs)
+    assert np.abs(a[:, 1:] - b[:, 1:]).max() < 1e-13          # spatial links
+    assert np.abs(a[:, 0] - b[:, 0]).max() < 1e-12            # temporal links via W
+    assert np.abs(a[:, 0] - U.reshape(size[0], 4, 3, 3, 2, Vs)[:, 0]).max() > 1e-3
+
+
+def test_coulomb_fix_every_slice(cuda):
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer
+
+    size = (4, 8, 8, 8)
+    U = np.concatenate([S.smooth_config((1,) + size[1:], 0.3, 80 + t)[0] for t in range(size[0])])
+    with GaugeFixer([size], gauge="coulomb", mixed=True) as gf:
+        gf.load(0, U)
+        reps = gf.fix(_sched(precision=1e-12, switch_theta=1e-9, check_precision=10, or_max_iter=5000))
+        g, a = gf.quality()
+    assert len(reps) == size[0]
+    assert all(r.converged and r.theta < 1e-12 for r in reps)
+    assert np.all(a < 1e-12)
+    # each slice against the oracle's Coulomb quality of the exported field
+    out = np.zeros_like(U)
+    with GaugeFixer([size], gauge="coulomb", mixed=True) as gf:
+        gf.load(0, U)
+        gf.fix(_sched(precision=1e-12, switch_theta=1e-9, check_precision=10, or_max_iter=5000))
+        gf.store(0, out)
+    Vs = int(np.prod(size[1:]))
+    for t in range(size[0]):
+        gq, aq = O.quality(out[t * Vs * 72:(t + 1) * Vs * 72].copy(), (1,) + size[1:], O.COULOMB)
+        assert aq < 1e-11
+        assert gq == pytest.approx(reps[t].gff, rel=1e-9)
