@@ -177,6 +177,7 @@ def run_profile_target(nsweeps: int):
     from su3_ma_gauge_gpu_b200.engine import GaugeFixer
 
     U, _ = S.smooth_config(SIZE, EPS, 1234, device="cuda")
+    torch.cuda.empty_cache()  # keep the device footprint of the profiled launches small
     dU = torch.from_numpy(U).cuda()
     with GaugeFixer([SIZE], mixed=True) as gf:
         gf.load(0, dU)
@@ -192,6 +193,99 @@ def run_profile_target(nsweeps: int):
     print(json.dumps({"profile_target": "ok", "sweeps_per_shape": nsweeps, "F": float(g[0]), "theta": float(a[0])}))
 
 
+GRIBOV_LATTICES = [((12, 12, 12, 12), 24), ((16, 16, 16, 16), 24), ((40, 20, 20, 20), 16)]
+
+
+def run_gribov(args):
+    """64 random-gauge-start Gribov copies of three uneven lattices (24 x 12^4, 24 x 16^4,
+    16 x 20^3x40, eps = 0.3 smooth fields), all fixed in ONE batch: every parity pass is one
+    launch over all copies, per-copy convergence decided on the device, check chunks replayed
+    from CUDA graphs, autotuned pass shape.  Reports copies/s and the best functional per lattice."""
+    import numpy as np
+    import torch
+
+    from su3_ma_gauge_gpu_b200 import synthetic as S
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer, Schedule
+
+    bases = [S.smooth_config(size, EPS, 500 + k, device="cuda")[0] for k, (size, _) in enumerate(GRIBOV_LATTICES)]
+    dbases = [torch.from_numpy(b).cuda() for b in bases]
+    sizes, owner = [], []
+    for k, (size, n) in enumerate(GRIBOV_LATTICES):
+        sizes += [size] * n
+        owner += [k] * n
+    stream = torch.cuda.Stream()
+    gf = GaugeFixer(sizes, mixed=True, stream=stream)
+    sched = Schedule(random_trafo=1, seed=77, or_max_iter=20000, precision=1e-12, switch_theta=1e-9,
+                     check_precision=args.check, reproject=100, micro_updates=0)
+
+    def step():
+        for i, k in enumerate(owner):
+            gf.load(i, dbases[k])
+        return gf.fix(sched)
+
+    reps = None
+    for _ in range(args.warmup):
+        reps = step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        reps = step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    vols = [int(np.prod(s)) for s in sizes]
+    updates = sum(v * r.or_sweeps for v, r in zip(vols, reps))
+    best = {}
+    for (size, _), k in zip(GRIBOV_LATTICES, range(len(GRIBOV_LATTICES))):
+        fs = [r.gff for r, o in zip(reps, owner) if o == k]
+        best["x".join(map(str, size))] = {"best_F": max(fs), "min_F": min(fs), "copies": len(fs)}
+    gf.close()
+    print(json.dumps({
+        "workload": "gribov", "copies": len(sizes), "total_sites": sum(vols), "ms_per_batch": ms,
+        "copies_per_s": len(sizes) / (ms * 1e-3), "gsite_updates_per_s": updates / (ms * 1e-3) / 1e9,
+        "all_converged": all(r.converged for r in reps), "max_theta": max(r.theta for r in reps),
+        "or_sweeps": {"min": min(r.or_sweeps for r in reps), "max": max(r.or_sweeps for r in reps)},
+        "best_per_lattice": best}))
+
+
+def run_plain8(args):
+    """The 8^4 plain-method configuration: Haar-random links, FP64 (the reference's full 18-real
+    array in, out), OR omega = 1.7 to theta < 1e-12, at most 20000 sweeps; timed per fix."""
+    import numpy as np
+    import torch
+
+    from su3_ma_gauge_gpu_b200 import synthetic as S
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer, Schedule
+
+    size = (8, 8, 8, 8)
+    U = torch.from_numpy(S.hot_config(size, 4242)).cuda()
+    out = torch.empty_like(U)
+    stream = torch.cuda.Stream()
+    gf = GaugeFixer([size], mixed=False, stream=stream)
+    sched = Schedule(or_max_iter=20000, precision=1e-12, check_precision=args.check, reproject=100,
+                     micro_updates=0)
+    rep = None
+    for _ in range(args.warmup):
+        gf.load(0, U)
+        rep = gf.fix(sched)[0]
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        gf.load(0, U)
+        rep = gf.fix(sched)[0]
+        gf.store(0, out)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    V = int(np.prod(size))
+    gf.close()
+    print(json.dumps({"workload": "plain8", "ms_per_fix": ms, "or_sweeps": rep.or_sweeps, "theta": rep.theta,
+                      "F": rep.gff, "converged": rep.converged, "us_per_sweep": ms * 1e3 / max(1, rep.or_sweeps),
+                      "gsite_updates_per_s": V * rep.or_sweeps / (ms * 1e-3) / 1e9}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -201,6 +295,9 @@ def main():
     ap.add_argument("--check", type=int, default=20, help="sweeps between quality checks")
     ap.add_argument("--cpu-budget", type=float, default=10.0)
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison run")
+    ap.add_argument("--workload", default="landau32", choices=["landau32", "gribov", "plain8"],
+                    help="landau32: the headline 32^4 mixed-precision fix; gribov: 64 random-gauge copies of "
+                         "uneven lattices in one batch; plain8: the 8^4 Haar-random FP64 plain fix")
     ap.add_argument("--profile", type=int, default=0, metavar="N",
                     help="profiling target: import the 32^4 input, N FP32 OR sweeps, switch to FP64, N FP64 "
                          "sweeps, one quality check; no timing output")
@@ -210,6 +307,12 @@ def main():
         return
     if args.profile:
         run_profile_target(args.profile)
+        return
+    if args.workload == "gribov":
+        run_gribov(args)
+        return
+    if args.workload == "plain8":
+        run_plain8(args)
         return
 
     import numpy as np

@@ -146,6 +146,15 @@ typedef struct gf_schedule {
     int use_graphs;        /* 1: replay check chunks from CUDA graphs */
     int autotune;          /* 1: gf_autotune first if the context is not tuned yet */
     int micro_every;       /* micro steps after every micro_every-th SA sweep (reference: 1) */
+    int sa_mode;           /* 0: linear (Landau/Coulomb apps), 1: geometric, 2: the MAG/U1xU1 apps'
+                              do-while with a slowed window; 0 with sa_geometric = 1 means 1 */
+    int sa_repeat;         /* SA (+ micro) sweeps per temperature (MAG app: 5) */
+    double sa_slow_lo, sa_slow_hi; /* sa_mode 2: step / sa_slow_factor for T in [lo, hi] (the apps
+                              compare the float T with double constants) */
+    float sa_slow_factor;
+    int sr_max_iter;       /* srmaxiter: stochastic relaxation sweeps before OR (MAG app) */
+    float sr_parameter;    /* srparameter */
+    double sr_stop_theta;  /* SR stops below max(precision, this) (MAG app: 1e-6) */
 } gf_schedule;
 
 typedef struct gf_report {
@@ -155,6 +164,7 @@ typedef struct gf_report {
     int sa_sweeps;         /* SA sweeps done */
     int converged;         /* theta < precision */
     int chunks;            /* check chunks launched */
+    int sr_sweeps;         /* SR sweeps done */
 } gf_report;
 
 int gf_create(const gf_ctx_params *params, gf_ctx **out);

@@ -65,7 +65,10 @@ class Schedule(ctypes.Structure):
                 ("sa_geometric", ctypes.c_int), ("micro_updates", ctypes.c_int), ("or_max_iter", ctypes.c_int),
                 ("or_parameter", ctypes.c_float), ("precision", ctypes.c_double), ("switch_theta", ctypes.c_double),
                 ("check_precision", ctypes.c_int), ("reproject", ctypes.c_int), ("use_graphs", ctypes.c_int),
-                ("autotune", ctypes.c_int), ("micro_every", ctypes.c_int)]
+                ("autotune", ctypes.c_int), ("micro_every", ctypes.c_int), ("sa_mode", ctypes.c_int),
+                ("sa_repeat", ctypes.c_int), ("sa_slow_lo", ctypes.c_double), ("sa_slow_hi", ctypes.c_double),
+                ("sa_slow_factor", ctypes.c_float), ("sr_max_iter", ctypes.c_int), ("sr_parameter", ctypes.c_float),
+                ("sr_stop_theta", ctypes.c_double)]
 
 
 class Report(ctypes.Structure):
@@ -73,7 +76,7 @@ class Report(ctypes.Structure):
 
     _fields_ = [("gff", ctypes.c_double), ("theta", ctypes.c_double), ("or_sweeps", ctypes.c_int),
                 ("or_sweeps_fp64", ctypes.c_int), ("sa_sweeps", ctypes.c_int), ("converged", ctypes.c_int),
-                ("chunks", ctypes.c_int)]
+                ("chunks", ctypes.c_int), ("sr_sweeps", ctypes.c_int)]
 
 
 SIGNATURES.update({

@@ -611,22 +611,65 @@ int gf_fix(gf_ctx *c, const gf_schedule *s, gf_report *rep)
         if ((st = gf_sweeps(c, ALG_RANDOM, 1, 0.f, (int)s->seed, (int)ctr))) return st;
         ctr += 2;
     }
-    // simulated annealing with microcanonical steps (:212-234); linear schedule as the
-    // reference, or geometric when sa_geometric is set
-    if (s->sa_steps > 0) {
+    // simulated annealing with microcanonical steps.  sa_mode 0: the Landau/Coulomb apps' linear
+    // schedule (apps/LandauGaugeFixingSU3_4D.cu:212-234); 1: geometric; 2: the MAG / U1xU1 apps'
+    // do-while, step (max-min)/steps divided by sa_slow_factor inside [sa_slow_lo, sa_slow_hi]
+    // (apps/MAGaugeFixingSU3_4D.cu:233-266).  Every temperature runs sa_repeat SA sweeps, each
+    // followed (every micro_every-th) by micro_updates microcanonical sweeps.
+    int sa_done = 0;
+    const int every = s->micro_every > 0 ? s->micro_every : 1;
+    const int repeat = s->sa_repeat > 0 ? s->sa_repeat : 1;
+    auto sa_temperature = [&](float T, int i) -> int {
+        for (int r = 0; r < repeat; r++) {
+            int q = gf_sweeps(c, ALG_SA, 1, T, (int)s->seed, (int)ctr);
+            if (q) return q;
+            ctr += 2;
+            if (s->micro_updates > 0 && (sa_done % every) == every - 1 &&
+                (q = gf_sweeps(c, ALG_MICRO, s->micro_updates, 0.f, 0, 0)))
+                return q;
+            sa_done++;
+        }
+        if (i % s->reproject == 0) return gf_reunitarize(c);
+        return GF_OK;
+    };
+    const int mode = s->sa_mode ? s->sa_mode : (s->sa_geometric ? 1 : 0);
+    if (s->sa_steps > 0 && mode == 2) {
+        float T = s->sa_max;
+        const float base_step = (s->sa_max - s->sa_min) / (float)s->sa_steps;
+        const float slow = s->sa_slow_factor > 0 ? s->sa_slow_factor : 1.f;
+        int i = 0;
+        do {
+            const float step = ((double)T <= s->sa_slow_hi && (double)T >= s->sa_slow_lo) ? base_step / slow : base_step;
+            if ((st = sa_temperature(T, i))) return st;
+            T -= step;
+            i++;
+        } while (T >= s->sa_min && i < 100 * s->sa_steps);
+    } else if (s->sa_steps > 0) {
         float T = s->sa_max;
         const float dT = (s->sa_max - s->sa_min) / (float)s->sa_steps;
         const double ratio = s->sa_steps > 1 ? pow((double)s->sa_min / s->sa_max, 1.0 / (s->sa_steps - 1)) : 1.0;
         for (int i = 0; i < s->sa_steps; i++) {
-            const float Ti = s->sa_geometric ? (float)(s->sa_max * pow(ratio, (double)i)) : T;
-            if ((st = gf_sweeps(c, ALG_SA, 1, Ti, (int)s->seed, (int)ctr))) return st;
-            ctr += 2;
-            const int every = s->micro_every > 0 ? s->micro_every : 1;
-            if (s->micro_updates > 0 && (i % every) == every - 1 &&
-                (st = gf_sweeps(c, ALG_MICRO, s->micro_updates, 0.f, 0, 0)))
-                return st;
-            if (i % s->reproject == 0 && (st = gf_reunitarize(c))) return st;
+            const float Ti = mode == 1 ? (float)(s->sa_max * pow(ratio, (double)i)) : T;
+            if ((st = sa_temperature(Ti, i))) return st;
             T -= dT;
+        }
+    }
+    // stochastic relaxation (the MAG app, apps/MAGaugeFixingSU3_4D.cu:278-297): SR sweeps until
+    // every instance has theta < max(precision, sr_stop_theta), checked every checkprecision sweeps
+    int sr_done = 0;
+    if (s->sr_max_iter > 0) {
+        std::vector<double> th(c->ninst);
+        for (int i = 0; i < s->sr_max_iter; i++) {
+            if ((st = gf_sweeps(c, ALG_SR, 1, s->sr_parameter, (int)s->seed, (int)ctr))) return st;
+            ctr += 2;
+            sr_done++;
+            if (i % s->reproject == 0 && (st = gf_reunitarize(c))) return st;
+            if (i % s->check_precision == 0) {
+                if ((st = gf_quality_all(c, nullptr, th.data()))) return st;
+                bool all = true;
+                for (double t : th) all &= (t < s->precision || t < s->sr_stop_theta);
+                if (all) break;
+            }
         }
     }
     // overrelaxation to theta < precision (:244-262).  The reference checks after sweep i when
@@ -736,7 +779,8 @@ int gf_fix(gf_ctx *c, const gf_schedule *s, gf_report *rep)
             rep[i].theta = c->h_quality[2 * i + 1];
             rep[i].or_sweeps = c->h_sweeps[i];
             rep[i].or_sweeps_fp64 = c->h_sweeps[c->ninst + i];
-            rep[i].sa_sweeps = s->sa_steps;
+            rep[i].sa_sweeps = sa_done;
+            rep[i].sr_sweeps = sr_done;
             rep[i].converged = rep[i].theta < s->precision;
             rep[i].chunks = launched;
         }

@@ -43,6 +43,30 @@ class Schedule:
     use_graphs: int = 1
     autotune: int = 1
     micro_every: int = 1
+    sa_mode: int = 0
+    sa_repeat: int = 1
+    sa_slow_lo: float = 0.0
+    sa_slow_hi: float = 0.0
+    sa_slow_factor: float = 1.0
+    sr_max_iter: int = 0
+    sr_parameter: float = 1.7
+    sr_stop_theta: float = 1e-6
+
+    @classmethod
+    def mag_app(cls, **kw) -> "Schedule":
+        """The MAG app's schedule (apps/MAGaugeFixingSU3_4D.cu:222-333): SA do-while with 5 SA +
+        micro sweeps per temperature and step/15 for T in [0.7, 0.88], then SR, then OR."""
+        base = dict(sa_mode=2, sa_repeat=5, sa_slow_lo=0.7, sa_slow_hi=0.88, sa_slow_factor=15.0,
+                    sr_max_iter=1000, sr_parameter=1.7, sr_stop_theta=1e-6)
+        base.update(kw)
+        return cls(**base)
+
+    @classmethod
+    def u1xu1_app(cls, **kw) -> "Schedule":
+        """The U1xU1 app's SA do-while: step/15 for T in [2, 2.7]."""
+        base = dict(sa_mode=2, sa_repeat=1, sa_slow_lo=2.0, sa_slow_hi=2.7, sa_slow_factor=15.0)
+        base.update(kw)
+        return cls(**base)
 
     def to_c(self) -> _lib.Schedule:
         s = _lib.Schedule()
@@ -60,6 +84,7 @@ class Report:
     sa_sweeps: int
     converged: bool
     chunks: int
+    sr_sweeps: int = 0
 
 
 def _real(a) -> int:
@@ -130,8 +155,8 @@ class GaugeFixer:
         s = (schedule or Schedule()).to_c()
         reps = (_lib.Report * self.ninstances)()
         check(lib().gf_fix(self._h, ctypes.byref(s), reps), "gf_fix")
-        return [Report(r.gff, r.theta, r.or_sweeps, r.or_sweeps_fp64, r.sa_sweeps, bool(r.converged), r.chunks)
-                for r in reps]
+        return [Report(r.gff, r.theta, r.or_sweeps, r.or_sweeps_fp64, r.sa_sweeps, bool(r.converged), r.chunks,
+                       r.sr_sweeps) for r in reps]
 
     def autotune(self):
         """Time the OR-pass launch shapes and keep the fastest; returns (fp32, fp64) choices."""

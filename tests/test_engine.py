@@ -148,13 +148,14 @@ def _mixed_vs_fp64(size, eps, seed):
 
 
 def test_fix_mixed_reaches_fp64_fixed_point(cuda):
-    """Mixed precision: FP32 bulk to 1e-9, FP64 polish to 1e-12.  On a field with a single basin
-    (eps = 0.1) it lands on the plain-FP64 maximum to 1e-10 relative in F."""
+    """Mixed precision: FP32 bulk to 1e-9, FP64 polish to 1e-12.  Rounding the links to FP32 is not
+    a gauge transformation, so the FP32 phase moves the field slightly off its gauge orbit: F
+    agrees with plain FP64 to the FP32 drift (1e-6 relative), not to 1e-10."""
     res, f0 = _mixed_vs_fp64((8, 8, 8, 8), 0.1, 2)
     assert res[False].converged and res[True].converged
     assert res[True].theta < 1e-12
     assert 0 < res[True].or_sweeps_fp64 < res[True].or_sweeps
-    assert res[True].gff == pytest.approx(res[False].gff, rel=1e-10)
+    assert res[True].gff == pytest.approx(res[False].gff, rel=1e-6)
     assert res[True].gff >= f0 - 1e-12  # fixing the transformed field recovers at least F(untransformed)
 
 
@@ -286,3 +287,36 @@ def test_coulomb_fix_every_slice(cuda):
         gq, aq = O.quality(out[t * Vs * 72:(t + 1) * Vs * 72].copy(), (1,) + size[1:], O.COULOMB)
         assert aq < 1e-11
         assert gq == pytest.approx(reps[t].gff, rel=1e-9)
+
+
+def _mag_app_temperatures(sa_steps, sa_min, sa_max, lo, hi, factor):
+    """Temperatures of the MAG app's do-while (apps/MAGaugeFixingSU3_4D.cu:233-266), in float32."""
+    f = np.float32
+    T, base = f(sa_max), f((f(sa_max) - f(sa_min)) / f(sa_steps))
+    out = []
+    while True:
+        step = base / f(factor) if (float(T) <= hi and float(T) >= lo) else base
+        out.append(float(T))
+        T = f(T - step)
+        if not T >= f(sa_min):
+            return out
+
+
+def test_mag_app_schedule(cuda):
+    """SA do-while with 5 sweeps per temperature and the slowed window, SR, then OR in mixed
+    precision, for MAG."""
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer, Schedule
+
+    size = (4, 4, 4, 8)
+    U, _ = S.smooth_config(size, 0.3, 90)
+    sch = Schedule.mag_app(sa_steps=20, sa_min=0.01, sa_max=1.4, micro_updates=1, or_max_iter=4000,
+                           precision=1e-12, switch_theta=1e-9, check_precision=10, reproject=20, seed=3)
+    temps = _mag_app_temperatures(20, 0.01, 1.4, 0.7, 0.88, 15.0)
+    with GaugeFixer([size], gauge="mag", mixed=True) as gf:
+        gf.load(0, U)
+        g0, _ = gf.quality()
+        rep = gf.fix(sch)[0]
+    assert rep.sa_sweeps == 5 * len(temps)
+    assert rep.sr_sweeps >= 1
+    assert rep.converged and rep.theta < 1e-12
+    assert rep.gff > g0[0]  # the MAG functional increased
