@@ -295,6 +295,9 @@ def main():
     ap.add_argument("--check", type=int, default=20, help="sweeps between quality checks")
     ap.add_argument("--cpu-budget", type=float, default=10.0)
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison run")
+    ap.add_argument("--mixed", default="refine", choices=["fast", "refine"],
+                    help="mixed-precision mode of the headline run: fast = FP32 storage converted to FP64 at "
+                         "the switch; refine = FP64 master + FP32 working copy + accumulated gauge transform")
     ap.add_argument("--workload", default="landau32", choices=["landau32", "gribov", "plain8"],
                     help="landau32: the headline 32^4 mixed-precision fix; gribov: 64 random-gauge copies of "
                          "uneven lattices in one batch; plain8: the 8^4 Haar-random FP64 plain fix")
@@ -396,7 +399,9 @@ def main():
     except Exception:
         pass
 
-    gf = GaugeFixer([SIZE], mixed=True, stream=stream)
+    mixed_mode = "refine" if args.mixed == "refine" else True
+    other_mode = True if args.mixed == "refine" else "refine"
+    gf = GaugeFixer([SIZE], mixed=mixed_mode, stream=stream)
     gf.load(0, dU_in)
     tuned = gf.autotune()  # launch shape of the OR pass per precision (0 = direct, else warps/block)
     clocks = ClockSampler(gpu_id)
@@ -418,6 +423,11 @@ def main():
 
     t32 = pass_ms()
     gf.close()
+
+    # the other mixed-precision mode, for the record
+    gfo = GaugeFixer([SIZE], mixed=other_mode, stream=stream)
+    ms_other, rep_other, _ = timed(gfo, step_resident, 1, 1)
+    gfo.close()
 
     res64 = None
     ms64 = None
@@ -483,8 +493,8 @@ def main():
         "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+f64", "data": "synthetic",
         "config": {"workload": "Landau gauge fix of a 32^4 SU(3) lattice to theta<1e-12: U=exp(i*0.3*H) under a "
-                               "seeded Haar gauge transform, OR omega=1.7, FP32 12-real storage to theta<1e-9 then "
-                               "FP64 polish; one step = import + gf_fix + export",
+                               "seeded Haar gauge transform, OR omega=1.7, FP32 12-real sweeps to theta<1e-9 then "
+                               f"FP64 polish ({args.mixed} mixed precision); one step = import + gf_fix + export",
                    "lattice": list(SIZE), "instances_per_gpu": 1, "check_every": args.check,
                    "l2": "inputs larger than L2 (FP32 field 201 MB, FP64 403 MB > 126 MB)"},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": V * 4 * 12 * 8, "d2h_bytes_per_step": V * 72 * 8,
@@ -494,9 +504,15 @@ def main():
         "cpu_baseline": cpu,
         "clocks": clk,
         "time_to_theta": {
+            "mixed_mode": args.mixed,
             "mixed_ms": ms_max, "fp64_ms": ms64,
             "fp64_over_mixed": (ms64 / ms_max) if ms64 else None,
             "mixed": {"or_sweeps": sweeps, "fp64_sweeps": n64, "theta": rep.theta, "F": rep.gff},
+            "other_mixed_mode": {"mode": "fast" if args.mixed == "refine" else "refine", "ms": ms_other,
+                                 "or_sweeps": rep_other.or_sweeps, "fp64_sweeps": rep_other.or_sweeps_fp64,
+                                 "theta": rep_other.theta, "F": rep_other.gff,
+                                 "F_rel_err_vs_fp64": (abs(rep_other.gff - res64.gff) / abs(res64.gff))
+                                 if res64 else None},
             "fp64": ({"or_sweeps": res64.or_sweeps, "theta": res64.theta, "F": res64.gff} if res64 else None),
             "F_rel_err_vs_fp64": (abs(rep.gff - res64.gff) / abs(res64.gff)) if res64 else None,
             "F_pre_transform": f0,

@@ -123,7 +123,11 @@ typedef struct gf_ctx_params {
     int gauge;             /* GF_LANDAU, GF_COULOMB, GF_MAG or GF_U1XU1 */
     int ninstances;        /* number of lattices, >= 1 */
     const int32_t *sizes;  /* 4 * ninstances extents {Nt, Nx, Ny, Nz}, all even */
-    int mixed;             /* 1: FP32 bulk + FP64 polish, 0: FP64 only */
+    int mixed;             /* 0: FP64 only; 1: FP32 storage for the bulk, converted to FP64 for the
+                              polish; 2 ("refine"): an FP64 master field plus an FP32 working copy
+                              that also accumulates the gauge transformation W(x); at the switch
+                              the master becomes W(x) U(x) W(x+mu)^dagger, so rounding in the FP32
+                              phase never moves the field off its gauge orbit */
     void *stream;          /* cudaStream_t to run on, or NULL for a stream of the context's own */
 } gf_ctx_params;
 
@@ -191,16 +195,43 @@ int gf_set_storage(gf_ctx *ctx, int real);
  * timeslice for GF_COULOMB), or NULL. */
 int gf_fix(gf_ctx *ctx, const gf_schedule *schedule, gf_report *reports);
 /* Autotuner: times the candidate launch shapes of the OR parity pass (one warp per 8-site tile;
- * pipelined with cp.async prefetch and 2, 4 or 8 warps per block) on a scratch copy of the
- * field and keeps the fastest per precision.  Outputs: 0 = direct, else warps per block of the
- * pipelined pass (-1: precision not used). */
+ * the same capped at 64 registers (FP32); pipelined with cp.async prefetch and 2, 4 or 8 warps
+ * per block) on a scratch copy of the field and keeps the fastest per precision.  Outputs: 0 =
+ * direct, 64 = direct with 64 registers, 2/4/8 = warps per block of the pipelined pass (-1:
+ * precision not used). */
 int gf_autotune(gf_ctx *ctx, int *choice_fp32, int *choice_fp64);
-/* Fix the launch shape instead: variant 0 (direct) or 1 (pipelined, warps = 2, 4 or 8). */
+/* Fix the launch shape instead: variant 0 (direct), 1 (pipelined, warps = 2, 4 or 8) or 2 (FP32
+ * direct capped at 64 registers). */
 int gf_set_pass_shape(gf_ctx *ctx, int real, int variant, int warps);
 /* Number of instances (lattices, or timeslices for GF_COULOMB). */
 int gf_instances(gf_ctx *ctx);
 /* Number of kernels this context has launched so far (each node of a replayed graph counts). */
 int gf_kernel_launches(gf_ctx *ctx, long long *count);
+
+/* ---- configuration files (lattice/LinkFile.hxx, lattice/filetypes/, apps/ildg.cpp, apps/qcdstag.cpp)
+ * Read a configuration into / write one from the GpuPattern array U (18 reals per link, like
+ * the plugin entry points) of the given precision, on the device (on_device = 1) or in host
+ * memory.  The payload is transcoded on the GPU in one pass.
+ *  GF_FILE_PLAIN       StandardPattern array of file_real reals, no header (LinkFile.hxx:83-167)
+ *  GF_FILE_HEADERONLY  header of (file size - payload) bytes, then PLAIN; on writing, the header
+ *                      is copied from template_path (FileHeaderOnly.hxx:72-103)
+ *  GF_FILE_VOGT        7 shorts {4, 3, Nt, Nx, Ny, Nz, sizeof(real)}, then PLAIN (FileVogt.hxx:60-108)
+ *  GF_FILE_ILDG        LIME container, "ildg-binary-data" in big-endian doubles, x fastest, file
+ *                      directions (x,y,z,t) = internal (1,2,3,0); on writing, every other record of
+ *                      template_path is copied and "xlf-info" gets " SA steps <sa_steps>" appended
+ *                      (apps/ildg.cpp:26-238)
+ *  GF_FILE_QCDSTAG     native doubles, direction-major, x fastest, directions as stored
+ *                      (apps/qcdstag.cpp:17-67)
+ * ILDG and QCDSTAG are always double; file_real is used by PLAIN / HEADERONLY / VOGT.  Blocking. */
+#define GF_FILE_PLAIN 0
+#define GF_FILE_HEADERONLY 1
+#define GF_FILE_VOGT 2
+#define GF_FILE_ILDG 3
+#define GF_FILE_QCDSTAG 4
+int gf_file_read(const char *path, int format, int file_real, const int32_t size[4], int real, void *U,
+                 int on_device, void *stream);
+int gf_file_write(const char *path, int format, int file_real, const int32_t size[4], int real, const void *U,
+                  int on_device, const char *template_path, int sa_steps, void *stream);
 
 #ifdef __cplusplus
 }

@@ -330,8 +330,20 @@ __device__ __forceinline__ R site_sum(R v)
 
 // One SU(2) subgroup step of GaugeFixingSubgroupStep::subgroup for the gauge GAUGE, done by the
 // lane that holds direction mu of the site (LANDAU/COULOMB :99-237, U1xU1 :238-353, MAG :354-589).
-template <int GAUGE, int ALGO, int I, int J, typename R>
-__device__ __forceinline__ void subgroup_step(Link<R> &up, Link<R> &dn, int mu, const AlgoParams &p, Rng<R> &rng)
+// A column of the site's accumulated gauge transformation W (refine mode): rows (I,J) <- g * rows.
+template <int I, int J, typename R>
+__device__ __forceinline__ void left_mult_column(Cx<R> (&col)[3], const R g[4])
+{
+    const Cx<R> a = col[I], b = col[J];
+    const Cx<R> p0 = cmul(cx<R>(g[0], g[3]), a), p1 = cmul(cx<R>(g[2], g[1]), b);
+    const Cx<R> q0 = cmul(cx<R>(-g[2], g[1]), a), q1 = cmul(cx<R>(g[0], -g[3]), b);
+    col[I] = cx<R>(p0.x + p1.x, p0.y + p1.y);
+    col[J] = cx<R>(q0.x + q1.x, q0.y + q1.y);
+}
+
+template <int GAUGE, int ALGO, int I, int J, typename R, bool SITE_W = false>
+__device__ __forceinline__ void subgroup_step(Link<R> &up, Link<R> &dn, int mu, const AlgoParams &p, Rng<R> &rng,
+                                              Cx<R> (*wcol)[3] = nullptr)
 {
     R w[4];
     if (GAUGE == MAG) {
@@ -385,15 +397,18 @@ __device__ __forceinline__ void subgroup_step(Link<R> &up, Link<R> &dn, int mu, 
     left_mult<I, J>(up, w);
     const R h[4] = {w[0], -w[1], -w[2], -w[3]};
     right_mult<I, J>(dn, h);
+    if (SITE_W) left_mult_column<I, J>(*wcol, w);
 }
 
-// the three subgroups in the reference order (0,2), (1,2), (0,1) (SU3::perSubgroup, SU3.hxx:762-771)
-template <int GAUGE, int ALGO, typename R>
-__device__ __forceinline__ void site_update(Link<R> &up, Link<R> &dn, int mu, const AlgoParams &p, Rng<R> &rng)
+// the three subgroups in the reference order (0,2), (1,2), (0,1) (SU3::perSubgroup, SU3.hxx:762-771);
+// with SITE_W the lane also left-multiplies its column of the site's accumulated W by every g
+template <int GAUGE, int ALGO, typename R, bool SITE_W = false>
+__device__ __forceinline__ void site_update(Link<R> &up, Link<R> &dn, int mu, const AlgoParams &p, Rng<R> &rng,
+                                            Cx<R> (*wcol)[3] = nullptr)
 {
-    subgroup_step<GAUGE, ALGO, 0, 2>(up, dn, mu, p, rng);
-    subgroup_step<GAUGE, ALGO, 1, 2>(up, dn, mu, p, rng);
-    subgroup_step<GAUGE, ALGO, 0, 1>(up, dn, mu, p, rng);
+    subgroup_step<GAUGE, ALGO, 0, 2, R, SITE_W>(up, dn, mu, p, rng, wcol);
+    subgroup_step<GAUGE, ALGO, 1, 2, R, SITE_W>(up, dn, mu, p, rng, wcol);
+    subgroup_step<GAUGE, ALGO, 0, 1, R, SITE_W>(up, dn, mu, p, rng, wcol);
 }
 
 // ---- lattice geometry -----------------------------------------------------------------------
@@ -458,6 +473,15 @@ __device__ __forceinline__ int64_t site_index(const Geom &g, const int32_t c[4])
 {
     const uint32_t l = (((uint32_t)c[0] * g.n[1] + c[1]) * g.n[2] + c[2]) * g.n[3] + c[3];
     return (int64_t)(l >> 1) + (((c[0] + c[1] + c[2] + c[3]) & 1) ? g.Vh : 0);
+}
+
+// forward neighbour x + mu of the site with coordinates c
+__device__ __forceinline__ int64_t neighbour_up(const Geom &g, const int32_t c[4], int mu)
+{
+    int32_t d[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) d[k] = (mu == k) ? ((c[k] + 1 == g.n[k]) ? 0 : c[k] + 1) : c[k];
+    return site_index(g, d);
 }
 
 // backward neighbour x - mu of the site with coordinates c (mu is lane-dependent, so the

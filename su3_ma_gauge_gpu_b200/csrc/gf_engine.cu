@@ -23,6 +23,8 @@ using namespace gfb;
 
 struct gf_ctx {
     int gauge = 0, ninst = 0, mixed = 0, device = 0;
+    int refine = 0;           // mixed mode 2: FP64 master + FP32 working copy + accumulated W
+    float2 *w = nullptr;      // refine: W of every instance (9 float2 planes of V each)
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     std::vector<InstDesc> h_inst;
@@ -115,7 +117,7 @@ template <typename R, int GAUGE, int ALGO>
 int launch_pass(const gf_ctx *c, const EngineDev &e, const PassArgs &a, const gf_ctx::PassShape &sh)
 {
     if constexpr (ALGO == ALG_OR) {
-        if (sh.variant == 1) {
+        if (sh.variant == 1 && !(sizeof(R) == 4 && c->refine)) {
             switch (sh.warps) {
             case 2: return launch_staged<R, GAUGE, ALGO, 2>(c, e, a, sh.blocks_per_sm);
             case 8: return launch_staged<R, GAUGE, ALGO, 8>(c, e, a, sh.blocks_per_sm);
@@ -124,6 +126,22 @@ int launch_pass(const gf_ctx *c, const EngineDev &e, const PassArgs &a, const gf
         }
     }
     const unsigned blocks = grid_for(a.c->total_warps * 32, 128);
+    if constexpr (sizeof(R) == 4) {
+        if (c->refine) {
+            if (sh.variant == 2)
+                k_batched_pass<R, GAUGE, ALGO, true, 8><<<blocks, 128, 0, a.c->stream>>>(e, a.c->total_warps,
+                                                                                      a.parity, a.p, a.want_state);
+            else
+                k_batched_pass<R, GAUGE, ALGO, true><<<blocks, 128, 0, a.c->stream>>>(e, a.c->total_warps, a.parity,
+                                                                                     a.p, a.want_state);
+            return launch_status("batched parity pass (refine)");
+        }
+        if (sh.variant == 2) {
+            k_batched_pass<R, GAUGE, ALGO, false, 8><<<blocks, 128, 0, a.c->stream>>>(e, a.c->total_warps, a.parity,
+                                                                                   a.p, a.want_state);
+            return launch_status("batched parity pass (64 registers)");
+        }
+    }
     k_batched_pass<R, GAUGE, ALGO><<<blocks, 128, 0, a.c->stream>>>(e, a.c->total_warps, a.parity, a.p,
                                                                      a.want_state);
     return launch_status("batched parity pass");
@@ -179,6 +197,18 @@ int launch_quality(const gf_ctx *c, const CheckParams &cp)
 int launch_reunitarise(const gf_ctx *c, int want_state, bool to64)
 {
     const unsigned blocks = grid_for(c->total_links, 256);
+    if (c->refine && to64) {
+        // refine switch: the FP64 master takes the accumulated W (an exact gauge transformation)
+        k_apply_w<<<blocks, 256, 0, c->stream>>>(c->dev(), c->total_links);
+        c->launches++;
+        return launch_status("apply W");
+    }
+    if (c->refine && want_state == ST_FP32) {
+        k_reunitarise_w<<<blocks, 256, 0, c->stream>>>(c->dev(), c->total_links, want_state);
+        c->launches++;
+        int st = launch_status("reunitarise W");
+        if (st) return st;
+    }
     if (to64)
         k_reunitarise<float, true><<<blocks, 256, 0, c->stream>>>(c->dev(), c->total_links, want_state);
     else if (want_state == ST_FP32)
@@ -266,6 +296,7 @@ int gf_create(const gf_ctx_params *p, gf_ctx **out)
     }
     c->gauge = p->gauge;
     c->mixed = p->mixed ? 1 : 0;
+    c->refine = p->mixed == 2 ? 1 : 0;
     cudaGetDevice(&c->device);
     cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device);
     const bool coulomb = p->gauge == GF_COULOMB;
@@ -297,6 +328,7 @@ int gf_create(const gf_ctx_params *p, gf_ctx **out)
         st = make_geom(inst_sizes[i].data(), p->gauge, coulomb, d.g);
         d.next = inst_next[i];
         d.t64 = coulomb ? reinterpret_cast<double2 *>(toff) : nullptr;  // rebased after allocation
+        d.w = reinterpret_cast<float2 *>(toff * 2);                       // 9 float2 per site < 12
         toff += 6 * d.g.V;
         d.warp_begin = woff;
         d.link_begin = loff;
@@ -338,11 +370,14 @@ int gf_create(const gf_ctx_params *p, gf_ctx **out)
     if ((st = cuda_status(cudaMalloc(&c->f64, n64 * sizeof(double2)), "cudaMalloc FP64 field"))) return fail(st);
     if (coulomb && (st = cuda_status(cudaMalloc(&c->t64, (size_t)toff * sizeof(double2)), "cudaMalloc temporal links")))
         return fail(st);
+    if (c->refine && (st = cuda_status(cudaMalloc(&c->w, (size_t)toff * 2 * sizeof(float2)), "cudaMalloc W")))
+        return fail(st);
     for (auto &d : c->h_inst) {
         const size_t off = (size_t)reinterpret_cast<uintptr_t>(d.f32);
         d.f32 = c->mixed ? c->f32 + off : nullptr;
         d.f64 = c->f64 + 2 * off;
         if (coulomb) d.t64 = c->t64 + (size_t)reinterpret_cast<uintptr_t>(d.t64);
+        d.w = c->refine ? c->w + (size_t)reinterpret_cast<uintptr_t>(d.w) : nullptr;
     }
     const int n = c->ninst;
     if ((st = cuda_status(cudaMalloc(&c->d_inst, sizeof(InstDesc) * n), "cudaMalloc"))) return fail(st);
@@ -388,6 +423,7 @@ int gf_destroy(gf_ctx *c)
     cudaFree(c->f32);
     cudaFree(c->f64);
     cudaFree(c->t64);
+    cudaFree(c->w);
     cudaFree(c->d_inst);
     cudaFree(c->d_state);
     cudaFree(c->d_quality);
@@ -449,7 +485,10 @@ int gf_import(gf_ctx *c, int lat, int real, const void *U, int on_host)
         const InstDesc &d = c->h_inst[i];
         const unsigned blocks = grid_for(4 * d.g.V, 256);
         const void *sp = src + (size_t)t * L.slice_reals * es;
-        if (target == ST_FP32) {
+        if (c->refine) {
+            if (real == GF_FP64) k_import_refine<double><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (const double *)sp);
+            else k_import_refine<float><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (const float *)sp);
+        } else if (target == ST_FP32) {
             if (real == GF_FP64) k_import<double, float><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (const double *)sp);
             else k_import<float, float><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (const float *)sp);
         } else {
@@ -500,6 +539,9 @@ int gf_export(gf_ctx *c, int lat, int real, void *U, int on_host)
         if (c->gauge == GF_COULOMB) {
             if (real == GF_FP64) k_export_coulomb<double><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (double *)dp);
             else k_export_coulomb<float><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (float *)dp);
+        } else if (c->h_state[c->ninst + i] == 0 && c->refine) {
+            if (real == GF_FP64) k_export_refine<double><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (double *)dp);
+            else k_export_refine<float><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (float *)dp);
         } else if (c->h_state[c->ninst + i] == 0) {
             if (real == GF_FP64) k_export<float, double><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (double *)dp);
             else k_export<float, float><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (float *)dp);
@@ -796,11 +838,16 @@ int gf_autotune(gf_ctx *c, int *choice_fp32, int *choice_fp64)
     clear_error();
     int st = check_ctx(c);
     if (st) return st;
-    static const gf_ctx::PassShape cands[] = {{0, 4, 0}, {1, 2, 0}, {1, 4, 0}, {1, 8, 0}};
-    // the pipelined pass does not implement the Coulomb W tracking: direct pass only
-    const int ncand = c->gauge == GF_COULOMB ? 1 : (int)(sizeof(cands) / sizeof(cands[0]));
+    // direct; pipelined with 2, 4, 8 warps per block; (FP32 only) direct capped at 64 registers
+    static const gf_ctx::PassShape cands64[] = {{0, 4, 0}, {1, 2, 0}, {1, 4, 0}, {1, 8, 0}};
+    static const gf_ctx::PassShape cands32[] = {{0, 4, 0}, {2, 4, 0}, {1, 2, 0}, {1, 4, 0}, {1, 8, 0}};
     for (int prec = 0; prec < 2; prec++) {
         if (prec == 0 && !c->mixed) continue;
+        const gf_ctx::PassShape *cands = prec == 0 ? cands32 : cands64;
+        // the pipelined pass implements neither the Coulomb W nor the refine W tracking
+        int ncand = prec == 0 ? 5 : 4;
+        if (c->gauge == GF_COULOMB) ncand = 1;
+        else if (prec == 0 && c->refine) ncand = 2;
         // scratch field, descriptors and states for this precision
         const InstDesc &last = c->h_inst.back();
         const size_t span32 = (size_t)(reinterpret_cast<const char *>(last.f32 ? last.f32 : (float4 *)nullptr) -
@@ -873,8 +920,9 @@ int gf_autotune(gf_ctx *c, int *choice_fp32, int *choice_fp64)
         c->shape[prec] = cands[besti];
         c->tuned[prec] = 1;
     }
-    if (choice_fp32) *choice_fp32 = c->mixed ? (c->shape[0].variant ? c->shape[0].warps : 0) : -1;
-    if (choice_fp64) *choice_fp64 = c->shape[1].variant ? c->shape[1].warps : 0;
+    auto code = [](const gf_ctx::PassShape &sh) { return sh.variant == 1 ? sh.warps : (sh.variant == 2 ? 64 : 0); };
+    if (choice_fp32) *choice_fp32 = c->mixed ? code(c->shape[0]) : -1;
+    if (choice_fp64) *choice_fp64 = code(c->shape[1]);
     return GF_OK;
 }
 
@@ -883,9 +931,10 @@ int gf_autotune(gf_ctx *c, int *choice_fp32, int *choice_fp64)
 int gf_set_pass_shape(gf_ctx *c, int real, int variant, int warps)
 {
     clear_error();
-    if (!c || !valid_real(real) || (variant != 0 && variant != 1) || (warps != 2 && warps != 4 && warps != 8) ||
-        (variant == 1 && c->gauge == GF_COULOMB)) {
-        set_error("invalid pass shape (Coulomb contexts use the direct pass)");
+    if (!c || !valid_real(real) || variant < 0 || variant > 2 || (warps != 2 && warps != 4 && warps != 8) ||
+        (variant == 1 && c->gauge == GF_COULOMB) || (variant == 1 && real == GF_FP32 && c->refine) ||
+        (variant == 2 && real == GF_FP64)) {
+        set_error("invalid pass shape (Coulomb and refine-FP32 passes are direct; the 64-register pass is FP32)");
         return GF_ERR_INVALID;
     }
     c->shape[real].variant = variant;

@@ -26,6 +26,7 @@ struct InstDesc {
     double2 *f64;         // packed FP64 field
     double2 *t64;         // Coulomb: the slice's original temporal links (6 double2 planes), else null
     int next;             // Coulomb: instance of timeslice t+1 of the same lattice, else -1
+    float2 *w;            // refine mode: accumulated gauge transformation, 9 float2 planes, else null
 };
 
 struct EngineDev {
@@ -65,9 +66,11 @@ __device__ __forceinline__ PackedField<double> packed_of<double>(const InstDesc 
 // One parity pass over every instance in state want_state.  A warp handles 8 sites of one
 // instance (instance ranges are whole warps).  seed_i = seed + instance, so instance 0 draws the
 // reference's Philox stream and the others draw independent ones.
-template <typename R, int GAUGE, int ALGO>
-__global__ void __launch_bounds__(128) k_batched_pass(EngineDev e, int64_t total_warps, int parity, AlgoParams p,
-                                                      int want_state)
+// MINB > 1 caps the registers (65536 / (128 * MINB) per thread) for more resident warps; the
+// autotuner decides whether the spills that may cost are worth it
+template <typename R, int GAUGE, int ALGO, bool SITE_W = false, int MINB = 1>
+__global__ void __launch_bounds__(128, MINB) k_batched_pass(EngineDev e, int64_t total_warps, int parity, AlgoParams p,
+                                                           int want_state)
 {
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (warp >= total_warps) return;
@@ -77,7 +80,156 @@ __global__ void __launch_bounds__(128) k_batched_pass(EngineDev e, int64_t total
     const PackedField<R> f = packed_of<R>(d);
     AlgoParams pi = p;
     pi.seed = p.seed + (uint32_t)i;
-    parity_pass_warp<R, GAUGE, ALGO, PackedField<R>, GAUGE == COULOMB>(f, f, d.g, warp - d.warp_begin, parity, pi);
+    parity_pass_warp<R, GAUGE, ALGO, PackedField<R>, GAUGE == COULOMB, SITE_W>(f, f, d.g, warp - d.warp_begin, parity,
+                                                                               pi, d.w);
+}
+
+// ---- refine mode: FP64 master + FP32 working copy + accumulated W --------------------------------
+__device__ __forceinline__ void load_w_f64(const InstDesc &d, int64_t s, Link<double> &W)
+{
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            const float2 v = d.w[(int64_t)(k * 3 + r) * d.g.V + s];
+            W.e[r][k] = cx<double>(v.x, v.y);
+        }
+}
+
+__device__ __forceinline__ void store_w(const InstDesc &d, int64_t s, const Link<double> &W)
+{
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+            d.w[(int64_t)(k * 3 + r) * d.g.V + s] = make_float2((float)W.e[r][k].x, (float)W.e[r][k].y);
+}
+
+// import of a refine instance: FP64 master and FP32 working copy of the links, W = 1
+template <typename Rin>
+__global__ void __launch_bounds__(256) k_import_refine(EngineDev e, int i, const Rin *U)
+{
+    const InstDesc d = e.inst[i];
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= 4 * d.g.V) return;
+    const int mu = (int)(idx / d.g.V);
+    const int64_t s = idx - mu * d.g.V;
+    Rin r[12];
+    RefField<Rin>{(Rin *)U, d.g.V}.load12(s, mu, r);
+    double m[12];
+    float f[12];
+#pragma unroll
+    for (int k = 0; k < 12; k++) {
+        m[k] = (double)r[k];
+        f[k] = (float)r[k];
+    }
+    packed_of<double>(d).store12(s, mu, m);
+    packed_of<float>(d).store12(s, mu, f);
+    if (mu == 0) {
+        Link<double> W;
+#pragma unroll
+        for (int a = 0; a < 3; a++)
+#pragma unroll
+            for (int b = 0; b < 3; b++) W.e[a][b] = cx<double>(a == b ? 1.0 : 0.0, 0.0);
+        store_w(d, s, W);
+    }
+}
+
+// reunitarise W (FP64 arithmetic) of every instance in state want_state
+__global__ void __launch_bounds__(256) k_reunitarise_w(EngineDev e, int64_t total_links, int want_state)
+{
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= total_links) return;
+    const int i = find_instance(e.inst, e.ninst, idx, [](const InstDesc &d) { return d.link_begin; });
+    if (e.state[i] != want_state) return;
+    const InstDesc d = e.inst[i];
+    const int64_t l = idx - d.link_begin;
+    if (l >= d.g.V) return;  // one thread per site: the first quarter of the instance's links
+    Link<double> W;
+    load_w_f64(d, l, W);
+    project_rows(W);
+    store_w(d, l, W);
+}
+
+// U64_mu(x) <- W(x) U64_mu(x) W(x+mu)^dagger, reunitarised, in FP64 (W reunitarised first)
+__device__ __forceinline__ void apply_w_link(const InstDesc &d, int64_t s, int mu, Link<double> &L)
+{
+    const int parity = s >= d.g.Vh;
+    int32_t c[4];
+    site_coords(d.g, s - (parity ? d.g.Vh : 0), parity, c);
+    const int64_t sf = neighbour_up(d.g, c, mu);
+    Link<double> W, Wf, T;
+    load_w_f64(d, s, W);
+    load_w_f64(d, sf, Wf);
+    project_rows(W);
+    project_rows(Wf);
+    load_link_f64<double>(packed_of<double>(d), s, mu, T);
+    Link<double> M;
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+            Cx<double> acc = cx<double>(0, 0);
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                const Cx<double> t = cmul(W.e[a][k], T.e[k][b]);
+                acc.x += t.x;
+                acc.y += t.y;
+            }
+            M.e[a][b] = acc;
+        }
+#pragma unroll
+    for (int a = 0; a < 2; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+            Cx<double> acc = cx<double>(0, 0);
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                const Cx<double> w = Wf.e[b][k];
+                const Cx<double> t = cmul(M.e[a][k], cx<double>(w.x, -w.y));
+                acc.x += t.x;
+                acc.y += t.y;
+            }
+            L.e[a][b] = acc;
+        }
+    project_rows(L);
+}
+
+// refine switch: the FP64 master of every instance in ST_SWITCH becomes W U64 W^dagger
+__global__ void __launch_bounds__(256) k_apply_w(EngineDev e, int64_t total_links)
+{
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= total_links) return;
+    const int i = find_instance(e.inst, e.ninst, idx, [](const InstDesc &d) { return d.link_begin; });
+    if (e.state[i] != ST_SWITCH) return;
+    const InstDesc d = e.inst[i];
+    const int64_t l = idx - d.link_begin;
+    const int mu = (int)(l / d.g.V);
+    const int64_t s = l - mu * d.g.V;
+    Link<double> L;
+    apply_w_link(d, s, mu, L);
+    double r[12];
+    pack12(L, r);
+    packed_of<double>(d).store12(s, mu, r);  // each thread reads and writes only its own link
+}
+
+// export of a refine instance still in FP32: W U64 W^dagger on the fly
+template <typename Rout>
+__global__ void __launch_bounds__(256) k_export_refine(EngineDev e, int i, Rout *U)
+{
+    const InstDesc d = e.inst[i];
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= 4 * d.g.V) return;
+    const int mu = (int)(idx / d.g.V);
+    const int64_t s = idx - mu * d.g.V;
+    Link<double> L;
+    apply_w_link(d, s, mu, L);
+    Link<Rout> o;
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) o.e[a][b] = cx<Rout>((Rout)L.e[a][b].x, (Rout)L.e[a][b].y);
+    RefField<Rout>{U, d.g.V}.store18(s, mu, o);
 }
 
 // ---- software-pipelined parity pass --------------------------------------------------------------

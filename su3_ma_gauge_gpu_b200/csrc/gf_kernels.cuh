@@ -22,9 +22,11 @@ __host__ __device__ constexpr double prefactor_gff_dev(int gauge) { return gauge
 // as U_0(t,x) <- W(t,x) U_0(t,x) W(t+1,x)^dagger (the product of the reference's per-sweep left and
 // right multiplications, CoulombKernelsSU3.hxx:226-247), so timeslices share no memory while they
 // sweep.
-template <typename R, int GAUGE, int ALGO, class F, bool TRACK_W = false>
+// W columns of the refine mode: float2 planes W[(k*3 + r)*V + s] = W(s)_{r,k}; lane mu < 3 of a
+// site carries column mu through the three subgroup steps (W <- g W), lane 3 carries none.
+template <typename R, int GAUGE, int ALGO, class F, bool TRACK_W = false, bool SITE_W = false>
 __device__ __forceinline__ void parity_pass_warp(const F &Fup, const F &Fdw, const Geom &g, int64_t warp, int parity,
-                                                 const AlgoParams &p)
+                                                 const AlgoParams &p, float2 *Wsite = nullptr)
 {
     const int lane = threadIdx.x & 31;
     const int mu = lane >> 3;
@@ -49,8 +51,21 @@ __device__ __forceinline__ void parity_pass_warp(const F &Fup, const F &Fdw, con
     }
     Rng<R> rng;
     if (ALGO == ALG_SA || ALGO == ALG_SR || ALGO == ALG_RANDOM) rng.init(ref_rng_tid(h), p.seed, p.counter);
-    site_update<GAUGE, ALGO>(up, dn, mu, p, rng);
+    Cx<R> wcol[3];
+    if (SITE_W) {
+        const int k = mu < 3 ? mu : 0;
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            const float2 v = Wsite[(int64_t)(k * 3 + r) * g.V + s];
+            wcol[r] = cx<R>((R)v.x, (R)v.y);
+        }
+    }
+    site_update<GAUGE, ALGO, R, SITE_W>(up, dn, mu, p, rng, &wcol);
     store_link<R>(Fup, s, mu, up);
+    if (SITE_W && mu < 3) {
+#pragma unroll
+        for (int r = 0; r < 3; r++) Wsite[(int64_t)(mu * 3 + r) * g.V + s] = make_float2((float)wcol[r].x, (float)wcol[r].y);
+    }
     if (wlane) return;
     if (tdown)
         store_link<R>(Fdw, sd, mu, dn);

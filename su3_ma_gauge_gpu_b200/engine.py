@@ -104,12 +104,16 @@ class GaugeFixer:
     reports and quality() are per timeslice."""
 
     def __init__(self, sizes, gauge="landau", mixed=True, stream=None):
+        """mixed: False (FP64 only), True (FP32 storage, then FP64), or "refine" (FP64 master,
+        FP32 working copy with the accumulated gauge transformation W applied to the master at
+        the switch: the FP32 phase never moves the field off its gauge orbit)."""
         self.sizes = [tuple(int(v) for v in s) for s in sizes]
         self.gauge = GAUGES[gauge] if isinstance(gauge, str) else int(gauge)
         arr = (ctypes.c_int32 * (4 * len(self.sizes)))(*[v for s in self.sizes for v in s])
         self._keep = arr
+        mode = 2 if mixed in ("refine", 2) else (1 if mixed else 0)
         p = _lib.CtxParams(self.gauge, len(self.sizes), ctypes.cast(arr, ctypes.POINTER(ctypes.c_int32)),
-                           1 if mixed else 0, stream.cuda_stream if stream is not None else None)
+                           mode, stream.cuda_stream if stream is not None else None)
         h = ctypes.c_void_p()
         check(lib().gf_create(ctypes.byref(p), ctypes.byref(h)), "gf_create")
         self._h = h
