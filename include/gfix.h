@@ -101,6 +101,19 @@ int gf_stats_create(int gauge, int real, const int32_t size[4], int stopping, gf
 int gf_stats_generate(gf_stats *st, const void *U, void *stream, double *gff, double *theta);
 int gf_stats_destroy(gf_stats *st);
 
+/* Gauge quality without any allocation.  No counterpart in the reference: it is
+ * gf_stats_generate for callers that cannot call cudaMalloc -- host frameworks that own all
+ * device memory through their own pool, or latency-critical loops where cudaMalloc's
+ * device-wide synchronisation is not acceptable.  Its reduction scratch is a fixed array in
+ * device memory (about 1 MiB, held by every GPU that loads the library until the process
+ * exits), so lattices are limited to 16,777,216 sites (64^4); larger ones return
+ * GF_ERR_INVALID.  The first call on a device looks up that array's device address (do it
+ * once before latency matters).  All calls share the one array: calls whose kernels overlap on
+ * the GPU (different streams or threads at the same time) race and must be serialised by the
+ * caller.  Blocking, like gf_stats_generate; stopping = GF_MAX or GF_AVERAGE. */
+int gf_quality_noalloc(int gauge, int real, const void *U, const int32_t size[4], int stopping,
+                       void *stream, double *gff, double *theta);
+
 /* ---- context level: batched, mixed-precision gauge fixing --------------------------------
  * A context holds one or more lattices ("instances": gauge copies, lattices of uneven extents)
  * in this library's packed 12-real layout.  Every parity pass is one launch over all instances;

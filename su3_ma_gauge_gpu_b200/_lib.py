@@ -47,6 +47,7 @@ SIGNATURES = {
     "gf_stats_create": (_c_int, [_c_int, _c_int, _i32p, _c_int, ctypes.POINTER(_vp)]),
     "gf_stats_generate": (_c_int, [_vp, _vp, _vp, _dp, _dp]),
     "gf_stats_destroy": (_c_int, [_vp]),
+    "gf_quality_noalloc": (_c_int, [_c_int, _c_int, _vp, _i32p, _c_int, _vp, _dp, _dp]),
     "gf_file_read": (_c_int, [ctypes.c_char_p, _c_int, _c_int, _i32p, _c_int, _vp, _c_int, _vp]),
     "gf_file_write": (_c_int, [ctypes.c_char_p, _c_int, _c_int, _i32p, _c_int, _vp, _c_int, ctypes.c_char_p, _c_int,
                                _vp]),
