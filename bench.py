@@ -167,10 +167,13 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def run_profile_target(nsweeps: int):
+def run_profile_target(nsweeps: int, mode: str = "fast"):
     """A short, fixed launch sequence of the hot kernels for ncu (see profiles/): the 32^4 input,
-    `nsweeps` OR sweeps with the direct pass and `nsweeps` with the pipelined pass (4 warps per
-    block), in FP32, then the same in FP64 -- 8 * nsweeps parity-pass launches in this order."""
+    `nsweeps` OR sweeps per launch shape in FP32, then the same in FP64.
+    mode "fast": FP32 storage; shapes direct, pipelined (4 warps per block) -- 8 * nsweeps
+    parity-pass launches.  mode "refine": FP64 master + FP32 working copy with W; FP32 shapes
+    direct, 64-register, register prefetch, then FP64 direct, pipelined (4), register prefetch --
+    12 * nsweeps parity-pass launches."""
     import torch
 
     from su3_ma_gauge_gpu_b200 import synthetic as S
@@ -179,18 +182,49 @@ def run_profile_target(nsweeps: int):
     U, _ = S.smooth_config(SIZE, EPS, 1234, device="cuda")
     torch.cuda.empty_cache()  # keep the device footprint of the profiled launches small
     dU = torch.from_numpy(U).cuda()
-    with GaugeFixer([SIZE], mixed=True) as gf:
+    shapes = {"fp32": (0, 1), "fp64": (0, 1)} if mode == "fast" else {"fp32": (0, 2, 3), "fp64": (0, 1, 3)}
+    with GaugeFixer([SIZE], mixed=True if mode == "fast" else "refine") as gf:
         gf.load(0, dU)
         for real in ("fp32", "fp64"):
             if real == "fp64":
                 gf.to_fp64()
-            for variant in (0, 1):
+            for variant in shapes[real]:
                 gf.set_pass_shape(real, variant, 4)
                 gf.sweeps("or", nsweeps, 1.7)
         g, a = gf.quality()
         gf.store(0, dU)
     torch.cuda.synchronize()
     print(json.dumps({"profile_target": "ok", "sweeps_per_shape": nsweeps, "F": float(g[0]), "theta": float(a[0])}))
+
+
+def run_launch_list(args):
+    """One step of the headline workload (import + gf_fix + export of the 32^4 field, the bench's
+    mixed mode and schedule) for a profiler's launch list: no warm-up, no clock sampling, and the
+    check chunks launched directly instead of replayed from CUDA graphs (the same kernels in the
+    same order).  Prints how many of the library's launches came before the step (autotuning)."""
+    import torch
+
+    from su3_ma_gauge_gpu_b200 import synthetic as S
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer, Schedule
+
+    U, _ = S.smooth_config(SIZE, EPS, 1234, device="cuda")
+    torch.cuda.empty_cache()
+    dU = torch.from_numpy(U).cuda()
+    out = torch.empty_like(dU)
+    sched = Schedule(or_max_iter=20000, precision=1e-12, switch_theta=args.switch_theta, check_precision=args.check,
+                     fold=args.fold, reproject=100, micro_updates=0, use_graphs=0)
+    with GaugeFixer([SIZE], mixed="refine" if args.mixed == "refine" else True) as gf:
+        gf.load(0, dU)
+        tuned = gf.autotune()
+        before = gf.kernel_launches()
+        gf.load(0, dU)
+        rep = gf.fix(sched)[0]
+        gf.store(0, out)
+        step = gf.kernel_launches() - before
+    torch.cuda.synchronize()
+    print(json.dumps({"launch_list": "ok", "launches_before_step": before, "launches_in_step": step,
+                      "launch_shape": tuned, "or_sweeps": rep.or_sweeps, "fp64_sweeps": rep.or_sweeps_fp64,
+                      "theta": rep.theta}))
 
 
 GRIBOV_LATTICES = [((12, 12, 12, 12), 24), ((16, 16, 16, 16), 24), ((40, 20, 20, 20), 16)]
@@ -294,6 +328,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--check", type=int, default=20, help="sweeps between quality checks")
     ap.add_argument("--cpu-budget", type=float, default=10.0)
+    ap.add_argument("--switch-theta", type=float, default=1e-9,
+                    help="theta at which the mixed run moves from FP32 sweeps to the FP64 polish")
+    ap.add_argument("--fold", type=int, default=1, choices=[0, 1],
+                    help="refine mode: 1 = iterative refinement below switch-theta (FP32 sweeps folded into "
+                         "the FP64 master after every check), 0 = FP64 polish sweeps")
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain FP64 comparison run")
     ap.add_argument("--mixed", default="refine", choices=["fast", "refine"],
                     help="mixed-precision mode of the headline run: fast = FP32 storage converted to FP64 at "
@@ -301,6 +340,9 @@ def main():
     ap.add_argument("--workload", default="landau32", choices=["landau32", "gribov", "plain8"],
                     help="landau32: the headline 32^4 mixed-precision fix; gribov: 64 random-gauge copies of "
                          "uneven lattices in one batch; plain8: the 8^4 Haar-random FP64 plain fix")
+    ap.add_argument("--profile-mode", default="fast", choices=["fast", "refine"])
+    ap.add_argument("--launch-list", action="store_true",
+                    help="one headline step without graphs, warm-up or clock sampling, for ncu's launch list")
     ap.add_argument("--profile", type=int, default=0, metavar="N",
                     help="profiling target: import the 32^4 input, N FP32 OR sweeps, switch to FP64, N FP64 "
                          "sweeps, one quality check; no timing output")
@@ -309,7 +351,10 @@ def main():
         run_reference(args)
         return
     if args.profile:
-        run_profile_target(args.profile)
+        run_profile_target(args.profile, args.profile_mode)
+        return
+    if args.launch_list:
+        run_launch_list(args)
         return
     if args.workload == "gribov":
         run_gribov(args)
@@ -343,7 +388,8 @@ def main():
     dU_in = U_pin.cuda()
     dU_out = torch.empty_like(dU_in)
     stream = torch.cuda.Stream()
-    sched = Schedule(or_max_iter=20000, precision=1e-12, switch_theta=1e-9, check_precision=args.check,
+    sched = Schedule(or_max_iter=20000, precision=1e-12, switch_theta=args.switch_theta, check_precision=args.check,
+                     fold=args.fold,
                      reproject=100, micro_updates=0)
 
     def barrier():
@@ -364,7 +410,7 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.SUM)
         return float(t.item())
 
-    def timed(gf, step_fn, steps, warmup):
+    def timed(gf, step_fn, steps, warmup, nvtx_name=None):
         reps = None
         for _ in range(warmup):
             reps = step_fn(gf)
@@ -373,8 +419,12 @@ def main():
         l0 = gf.kernel_launches()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
+        if nvtx_name:  # lets a profiler's launch list select exactly the timed steps
+            torch.cuda.nvtx.range_push(nvtx_name)
         for _ in range(steps):
             reps = step_fn(gf)
+        if nvtx_name:
+            torch.cuda.nvtx.range_pop()
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
@@ -405,7 +455,7 @@ def main():
     gf.load(0, dU_in)
     tuned = gf.autotune()  # launch shape of the OR pass per precision (0 = direct, else warps/block)
     clocks = ClockSampler(gpu_id)
-    ms, rep, launches = timed(gf, step_resident, args.steps, args.warmup)
+    ms, rep, launches = timed(gf, step_resident, args.steps, args.warmup, nvtx_name="timed_steps")
     clk = clocks.stop()
     ms_e2e, rep_e2e, _ = timed(gf, step_host, max(1, args.steps - 1), 1)
 
@@ -493,8 +543,12 @@ def main():
         "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32+f64", "data": "synthetic",
         "config": {"workload": "Landau gauge fix of a 32^4 SU(3) lattice to theta<1e-12: U=exp(i*0.3*H) under a "
-                               "seeded Haar gauge transform, OR omega=1.7, FP32 12-real sweeps to theta<1e-9 then "
-                               f"FP64 polish ({args.mixed} mixed precision); one step = import + gf_fix + export",
+                               "seeded Haar gauge transform, OR omega=1.7, FP32 12-real sweeps to "
+                               f"theta<{args.switch_theta:g}, then "
+                               + ("iterative refinement to theta<1e-12 (FP32 sweeps folded into an FP64 master "
+                                  "after every check, theta measured on the master in FP64)"
+                                  if args.mixed == "refine" and args.fold else "FP64 polish sweeps to theta<1e-12")
+                               + f" ({args.mixed} mixed precision); one step = import + gf_fix + export",
                    "lattice": list(SIZE), "instances_per_gpu": 1, "check_every": args.check,
                    "l2": "inputs larger than L2 (FP32 field 201 MB, FP64 403 MB > 126 MB)"},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": V * 4 * 12 * 8, "d2h_bytes_per_step": V * 72 * 8,
@@ -504,7 +558,7 @@ def main():
         "cpu_baseline": cpu,
         "clocks": clk,
         "time_to_theta": {
-            "mixed_mode": args.mixed,
+            "mixed_mode": args.mixed, "fold": args.fold, "switch_theta": args.switch_theta,
             "mixed_ms": ms_max, "fp64_ms": ms64,
             "fp64_over_mixed": (ms64 / ms_max) if ms64 else None,
             "mixed": {"or_sweeps": sweeps, "fp64_sweeps": n64, "theta": rep.theta, "F": rep.gff},

@@ -140,7 +140,8 @@ typedef struct gf_ctx_params {
                               polish; 2 ("refine"): an FP64 master field plus an FP32 working copy
                               that also accumulates the gauge transformation W(x); at the switch
                               the master becomes W(x) U(x) W(x+mu)^dagger, so rounding in the FP32
-                              phase never moves the field off its gauge orbit */
+                              phase never moves the field off its gauge orbit (not for GF_COULOMB:
+                              GF_ERR_UNSUPPORTED) */
     void *stream;          /* cudaStream_t to run on, or NULL for a stream of the context's own */
 } gf_ctx_params;
 
@@ -172,6 +173,16 @@ typedef struct gf_schedule {
     int sr_max_iter;       /* srmaxiter: stochastic relaxation sweeps before OR (MAG app) */
     float sr_parameter;    /* srparameter */
     double sr_stop_theta;  /* SR stops below max(precision, this) (MAG app: 1e-6) */
+    int stall_checks;      /* mixed contexts: an FP32 instance also moves to FP64 after this many
+                              checks in a row without theta falling below 0.98 x its best FP32
+                              theta -- FP32 rounding has become the floor (MAG's theta stalls
+                              near 2e-7 in FP32, far above any useful switch_theta); 0: off */
+    int fold;              /* refine contexts (mixed = 2): 1 = iterative refinement -- below
+                              switch_theta the FP32 working copy keeps sweeping, and after every
+                              check W is folded into the FP64 master (U64 <- W U64 W^dagger), the
+                              working copy restarts from the master, and theta is measured on the
+                              master in FP64; FP64 sweeps only if folds stop gaining (stall_checks).
+                              0 = switch to FP64 sweeps at switch_theta */
 } gf_schedule;
 
 typedef struct gf_report {
@@ -208,13 +219,14 @@ int gf_set_storage(gf_ctx *ctx, int real);
  * timeslice for GF_COULOMB), or NULL. */
 int gf_fix(gf_ctx *ctx, const gf_schedule *schedule, gf_report *reports);
 /* Autotuner: times the candidate launch shapes of the OR parity pass (one warp per 8-site tile;
- * the same capped at 64 registers (FP32); pipelined with cp.async prefetch and 2, 4 or 8 warps
- * per block) on a scratch copy of the field and keeps the fastest per precision.  Outputs: 0 =
- * direct, 64 = direct with 64 registers, 2/4/8 = warps per block of the pipelined pass (-1:
- * precision not used). */
+ * the same capped at 64 registers (FP32); persistent with the next tile prefetched into
+ * registers; pipelined with cp.async prefetch and 2, 4 or 8 warps per block) on a scratch copy
+ * of the field (and of W in refine contexts) and keeps the fastest per precision.  Outputs: 0 =
+ * direct, 64 = direct with 64 registers, 100 = register prefetch, 2/4/8 = warps per block of the
+ * pipelined pass (-1: precision not used). */
 int gf_autotune(gf_ctx *ctx, int *choice_fp32, int *choice_fp64);
-/* Fix the launch shape instead: variant 0 (direct), 1 (pipelined, warps = 2, 4 or 8) or 2 (FP32
- * direct capped at 64 registers). */
+/* Fix the launch shape instead: variant 0 (direct), 1 (pipelined, warps = 2, 4 or 8), 2 (FP32
+ * direct capped at 64 registers) or 3 (register prefetch).  GF_COULOMB: 0 or 2; refine FP32: not 1. */
 int gf_set_pass_shape(gf_ctx *ctx, int real, int variant, int warps);
 /* Number of instances (lattices, or timeslices for GF_COULOMB). */
 int gf_instances(gf_ctx *ctx);

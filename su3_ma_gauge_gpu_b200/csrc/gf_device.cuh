@@ -330,15 +330,22 @@ __device__ __forceinline__ R site_sum(R v)
 
 // One SU(2) subgroup step of GaugeFixingSubgroupStep::subgroup for the gauge GAUGE, done by the
 // lane that holds direction mu of the site (LANDAU/COULOMB :99-237, U1xU1 :238-353, MAG :354-589).
-// A column of the site's accumulated gauge transformation W (refine mode): rows (I,J) <- g * rows.
+// Refine mode: column k of D = W - 1, the deviation of the site's accumulated gauge
+// transformation from the identity, under W <- g W:  D' = D + (g - 1)(1 + D) on rows (I, J).
+// g - 1 is formed without cancellation (g0 - 1 = -|g_vec|^2 / (1 + g0)), so near convergence, where
+// the folds keep W close to 1, D carries the small rotations to FP32 relative accuracy instead of
+// rounding them against the unit diagonal.
 template <int I, int J, typename R>
-__device__ __forceinline__ void left_mult_column(Cx<R> (&col)[3], const R g[4])
+__device__ __forceinline__ void left_mult_dcolumn(Cx<R> (&col)[3], const R g[4], int k)
 {
-    const Cx<R> a = col[I], b = col[J];
-    const Cx<R> p0 = cmul(cx<R>(g[0], g[3]), a), p1 = cmul(cx<R>(g[2], g[1]), b);
-    const Cx<R> q0 = cmul(cx<R>(-g[2], g[1]), a), q1 = cmul(cx<R>(g[0], -g[3]), b);
-    col[I] = cx<R>(p0.x + p1.x, p0.y + p1.y);
-    col[J] = cx<R>(q0.x + q1.x, q0.y + q1.y);
+    const R v2 = g[1] * g[1] + g[2] * g[2] + g[3] * g[3];
+    const R em = g[0] >= (R)0 ? -v2 / ((R)1 + g[0]) : g[0] - (R)1;
+    const Cx<R> a = cx<R>(col[I].x + (k == I ? (R)1 : (R)0), col[I].y);
+    const Cx<R> b = cx<R>(col[J].x + (k == J ? (R)1 : (R)0), col[J].y);
+    const Cx<R> p0 = cmul(cx<R>(em, g[3]), a), p1 = cmul(cx<R>(g[2], g[1]), b);
+    const Cx<R> q0 = cmul(cx<R>(-g[2], g[1]), a), q1 = cmul(cx<R>(em, -g[3]), b);
+    col[I] = cx<R>(col[I].x + (p0.x + p1.x), col[I].y + (p0.y + p1.y));
+    col[J] = cx<R>(col[J].x + (q0.x + q1.x), col[J].y + (q0.y + q1.y));
 }
 
 template <int GAUGE, int ALGO, int I, int J, typename R, bool SITE_W = false>
@@ -397,11 +404,11 @@ __device__ __forceinline__ void subgroup_step(Link<R> &up, Link<R> &dn, int mu, 
     left_mult<I, J>(up, w);
     const R h[4] = {w[0], -w[1], -w[2], -w[3]};
     right_mult<I, J>(dn, h);
-    if (SITE_W) left_mult_column<I, J>(*wcol, w);
+    if (SITE_W) left_mult_dcolumn<I, J>(*wcol, w, mu & 1);
 }
 
 // the three subgroups in the reference order (0,2), (1,2), (0,1) (SU3::perSubgroup, SU3.hxx:762-771);
-// with SITE_W the lane also left-multiplies its column of the site's accumulated W by every g
+// with SITE_W the lane also applies every g to its column (mu & 1) of the site's D = W - 1
 template <int GAUGE, int ALGO, typename R, bool SITE_W = false>
 __device__ __forceinline__ void site_update(Link<R> &up, Link<R> &dn, int mu, const AlgoParams &p, Rng<R> &rng,
                                             Cx<R> (*wcol)[3] = nullptr)

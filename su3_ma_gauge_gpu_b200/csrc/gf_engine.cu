@@ -24,7 +24,7 @@ using namespace gfb;
 struct gf_ctx {
     int gauge = 0, ninst = 0, mixed = 0, device = 0;
     int refine = 0;           // mixed mode 2: FP64 master + FP32 working copy + accumulated W
-    float2 *w = nullptr;      // refine: W of every instance (9 float2 planes of V each)
+    float2 *w = nullptr;      // refine: columns 0, 1 of W of every instance (6 float2 planes of V each)
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     std::vector<InstDesc> h_inst;
@@ -71,6 +71,8 @@ struct gf_ctx {
         e.quality = d_quality;
         e.partials = d_partials;
         e.tickets = d_tickets;
+        e.best32 = d_quality + 2 * ninst;
+        e.stall = d_state + 4 * ninst;
         return e;
     }
 };
@@ -113,9 +115,37 @@ int launch_staged(const gf_ctx *c, const EngineDev &e, const PassArgs &a, int bl
     return launch_status("batched parity pass (pipelined)");
 }
 
+template <typename R, int GAUGE, int ALGO, bool SITE_W>
+int launch_rp(const gf_ctx *c, const EngineDev &e, const PassArgs &a, int blocks_per_sm)
+{
+    auto kern = k_batched_pass_rp<R, GAUGE, ALGO, SITE_W>;
+    static int occ_cached = 0;  // resident blocks per SM of this instantiation
+    int occ = blocks_per_sm;
+    if (occ <= 0) {
+        if (occ_cached <= 0) {
+            int o = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, 128, 0) != cudaSuccess || o < 1) o = 1;
+            occ_cached = o;
+        }
+        occ = occ_cached;
+    }
+    const int64_t need = (a.c->total_warps + 3) / 4;
+    const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)c->num_sms * occ));
+    kern<<<blocks, 128, 0, a.c->stream>>>(e, a.c->total_warps, a.parity, a.p, a.want_state);
+    return launch_status("batched parity pass (register prefetch)");
+}
+
 template <typename R, int GAUGE, int ALGO>
 int launch_pass(const gf_ctx *c, const EngineDev &e, const PassArgs &a, const gf_ctx::PassShape &sh)
 {
+    if constexpr (ALGO == ALG_OR && GAUGE != COULOMB) {
+        if (sh.variant == 3) {
+            if constexpr (sizeof(R) == 4) {
+                if (c->refine) return launch_rp<R, GAUGE, ALGO, true>(c, e, a, sh.blocks_per_sm);
+            }
+            return launch_rp<R, GAUGE, ALGO, false>(c, e, a, sh.blocks_per_sm);
+        }
+    }
     if constexpr (ALGO == ALG_OR) {
         if (sh.variant == 1 && !(sizeof(R) == 4 && c->refine)) {
             switch (sh.warps) {
@@ -269,6 +299,19 @@ int enqueue_or_chunk(gf_ctx *c, int nsweeps, float omega, bool reproject, const 
     if (has32) {
         cp.want_state = ST_FP32;
         if ((st = launch_quality(c, cp))) return st;
+        if (c->refine && cp.fold) {
+            // iterative refinement: instances now in ST_FOLD fold W into the FP64 master, restart
+            // the working copy, and are checked on the master (their sweeps are already counted)
+            const unsigned blocks = grid_for(c->total_links, 256);
+            k_fold_apply<<<blocks, 256, 0, c->stream>>>(c->dev(), c->total_links);
+            k_fold_reset_w<<<blocks, 256, 0, c->stream>>>(c->dev(), c->total_links);
+            c->launches += 2;
+            if ((st = launch_status("fold"))) return st;
+            CheckParams cf = cp;
+            cf.want_state = ST_FOLD;
+            cf.chunk_sweeps = 0;
+            if ((st = launch_quality(c, cf))) return st;
+        }
         if ((st = launch_reunitarise(c, ST_SWITCH, true))) return st;
         k_finish_switch<<<grid_for(c->ninst, 128), 128, 0, c->stream>>>(c->dev());
         c->launches++;
@@ -286,6 +329,15 @@ int gf_create(const gf_ctx_params *p, gf_ctx **out)
     clear_error();
     if (!p || !out || p->ninstances < 1 || !p->sizes || !valid_gauge(p->gauge)) {
         set_error("invalid gf_ctx_params");
+        return GF_ERR_INVALID;
+    }
+    if (p->mixed == 2 && p->gauge == GF_COULOMB) {
+        // a Coulomb slice already keeps its gauge transformation in its temporal planes
+        set_error("refine mode (mixed = 2) is not available for GF_COULOMB; use mixed = 1");
+        return GF_ERR_UNSUPPORTED;
+    }
+    if (p->mixed < 0 || p->mixed > 2) {
+        set_error("mixed must be 0, 1 or 2");
         return GF_ERR_INVALID;
     }
     *out = nullptr;
@@ -328,7 +380,7 @@ int gf_create(const gf_ctx_params *p, gf_ctx **out)
         st = make_geom(inst_sizes[i].data(), p->gauge, coulomb, d.g);
         d.next = inst_next[i];
         d.t64 = coulomb ? reinterpret_cast<double2 *>(toff) : nullptr;  // rebased after allocation
-        d.w = reinterpret_cast<float2 *>(toff * 2);                       // 9 float2 per site < 12
+        d.w = reinterpret_cast<float2 *>(toff);                           // 2 columns: 6 float2 per site
         toff += 6 * d.g.V;
         d.warp_begin = woff;
         d.link_begin = loff;
@@ -370,7 +422,7 @@ int gf_create(const gf_ctx_params *p, gf_ctx **out)
     if ((st = cuda_status(cudaMalloc(&c->f64, n64 * sizeof(double2)), "cudaMalloc FP64 field"))) return fail(st);
     if (coulomb && (st = cuda_status(cudaMalloc(&c->t64, (size_t)toff * sizeof(double2)), "cudaMalloc temporal links")))
         return fail(st);
-    if (c->refine && (st = cuda_status(cudaMalloc(&c->w, (size_t)toff * 2 * sizeof(float2)), "cudaMalloc W")))
+    if (c->refine && (st = cuda_status(cudaMalloc(&c->w, (size_t)toff * sizeof(float2)), "cudaMalloc W")))
         return fail(st);
     for (auto &d : c->h_inst) {
         const size_t off = (size_t)reinterpret_cast<uintptr_t>(d.f32);
@@ -381,11 +433,13 @@ int gf_create(const gf_ctx_params *p, gf_ctx **out)
     }
     const int n = c->ninst;
     if ((st = cuda_status(cudaMalloc(&c->d_inst, sizeof(InstDesc) * n), "cudaMalloc"))) return fail(st);
-    if ((st = cuda_status(cudaMalloc(&c->d_state, sizeof(int) * 4 * n), "cudaMalloc"))) return fail(st);
+    // state, storage, sweeps, sweeps64, stall
+    if ((st = cuda_status(cudaMalloc(&c->d_state, sizeof(int) * 5 * n), "cudaMalloc"))) return fail(st);
     c->d_storage = c->d_state + n;
     c->d_sweeps = c->d_state + 2 * n;
     c->d_sweeps64 = c->d_state + 3 * n;
-    if ((st = cuda_status(cudaMalloc(&c->d_quality, sizeof(double) * 2 * n), "cudaMalloc"))) return fail(st);
+    // functional, theta, best FP32 theta
+    if ((st = cuda_status(cudaMalloc(&c->d_quality, sizeof(double) * 3 * n), "cudaMalloc"))) return fail(st);
     if ((st = cuda_status(cudaMalloc(&c->d_partials, sizeof(double) * 2 * c->total_qblocks), "cudaMalloc")))
         return fail(st);
     if ((st = cuda_status(cudaMalloc(&c->d_tickets, sizeof(unsigned) * n), "cudaMalloc"))) return fail(st);
@@ -402,12 +456,12 @@ int gf_create(const gf_ctx_params *p, gf_ctx **out)
     if ((st = cuda_status(cudaMemcpyAsync(c->d_inst, c->h_inst.data(), sizeof(InstDesc) * n, cudaMemcpyHostToDevice,
                                           c->stream), "descriptor copy")))
         return fail(st);
-    std::vector<int> init(4 * n, 0);
+    std::vector<int> init(5 * n, 0);
     for (int i = 0; i < n; i++) {
         init[i] = ST_DONE;                 // nothing imported yet
         init[n + i] = c->mixed ? 0 : 1;    // storage
     }
-    if ((st = cuda_status(cudaMemcpyAsync(c->d_state, init.data(), sizeof(int) * 4 * n, cudaMemcpyHostToDevice,
+    if ((st = cuda_status(cudaMemcpyAsync(c->d_state, init.data(), sizeof(int) * 5 * n, cudaMemcpyHostToDevice,
                                           c->stream), "state init")))
         return fail(st);
     if ((st = cuda_status(cudaMemsetAsync(c->d_tickets, 0, sizeof(unsigned) * n, c->stream), "memset"))) return fail(st);
@@ -723,6 +777,8 @@ int gf_fix(gf_ctx *c, const gf_schedule *s, gf_report *rep)
     base.switch_theta = c->mixed ? s->switch_theta : -1.0;
     base.precision = s->precision;
     base.stop_max = 0;
+    base.stall_checks = s->stall_checks;
+    base.fold = c->refine ? s->fold : 0;
     {
         std::vector<int> zeros(2 * c->ninst, 0);
         if ((st = cuda_status(cudaMemcpyAsync(c->d_sweeps, zeros.data(), sizeof(int) * 2 * c->ninst,
@@ -838,16 +894,17 @@ int gf_autotune(gf_ctx *c, int *choice_fp32, int *choice_fp64)
     clear_error();
     int st = check_ctx(c);
     if (st) return st;
-    // direct; pipelined with 2, 4, 8 warps per block; (FP32 only) direct capped at 64 registers
-    static const gf_ctx::PassShape cands64[] = {{0, 4, 0}, {1, 2, 0}, {1, 4, 0}, {1, 8, 0}};
-    static const gf_ctx::PassShape cands32[] = {{0, 4, 0}, {2, 4, 0}, {1, 2, 0}, {1, 4, 0}, {1, 8, 0}};
+    // direct; register prefetch (persistent); pipelined with 2, 4, 8 warps per block; (FP32 only)
+    // direct capped at 64 registers.  Coulomb passes are direct only, refine-FP32 passes (W
+    // tracking) direct, 64-register or register prefetch.
+    static const gf_ctx::PassShape cands64[] = {{0, 4, 0}, {3, 4, 0}, {1, 2, 0}, {1, 4, 0}, {1, 8, 0}};
+    static const gf_ctx::PassShape cands32[] = {{0, 4, 0}, {2, 4, 0}, {3, 4, 0}, {1, 2, 0}, {1, 4, 0}, {1, 8, 0}};
     for (int prec = 0; prec < 2; prec++) {
         if (prec == 0 && !c->mixed) continue;
         const gf_ctx::PassShape *cands = prec == 0 ? cands32 : cands64;
-        // the pipelined pass implements neither the Coulomb W nor the refine W tracking
-        int ncand = prec == 0 ? 5 : 4;
+        int ncand = prec == 0 ? 6 : 5;
         if (c->gauge == GF_COULOMB) ncand = 1;
-        else if (prec == 0 && c->refine) ncand = 2;
+        else if (prec == 0 && c->refine) ncand = 3;
         // scratch field, descriptors and states for this precision
         const InstDesc &last = c->h_inst.back();
         const size_t span32 = (size_t)(reinterpret_cast<const char *>(last.f32 ? last.f32 : (float4 *)nullptr) -
@@ -858,11 +915,13 @@ int gf_autotune(gf_ctx *c, int *choice_fp32, int *choice_fp64)
                               (size_t)24 * last.g.V * sizeof(double2);
         const size_t span = prec == 0 ? span32 : span64;
         void *scratch = nullptr;
+        float2 *wscratch = nullptr;  // refine: the passes also update W, which must not be touched
         InstDesc *dinst = nullptr;
         int *dstate = nullptr;
         cudaEvent_t e0 = nullptr, e1 = nullptr;
         auto cleanup = [&]() {
             cudaFree(scratch);
+            cudaFree(wscratch);
             cudaFree(dinst);
             cudaFree(dstate);
             if (e0) cudaEventDestroy(e0);
@@ -875,6 +934,15 @@ int gf_autotune(gf_ctx *c, int *choice_fp32, int *choice_fp64)
         const void *src = prec == 0 ? (const void *)c->f32 : (const void *)c->f64;
         cudaMemcpyAsync(scratch, src, span, cudaMemcpyDeviceToDevice, c->stream);
         std::vector<InstDesc> hi = c->h_inst;
+        if (prec == 0 && c->refine) {
+            const size_t spanw = (size_t)(last.w - c->w) + (size_t)6 * last.g.V;  // float2 count
+            if ((st = cuda_status(cudaMalloc(&wscratch, spanw * sizeof(float2)), "autotune W scratch"))) {
+                cleanup();
+                return st;
+            }
+            cudaMemcpyAsync(wscratch, c->w, spanw * sizeof(float2), cudaMemcpyDeviceToDevice, c->stream);
+            for (auto &d : hi) d.w = wscratch + (d.w - c->w);
+        }
         for (auto &d : hi) {
             if (prec == 0)
                 d.f32 = reinterpret_cast<float4 *>((char *)scratch + ((char *)d.f32 - (char *)c->f32));
@@ -920,21 +988,25 @@ int gf_autotune(gf_ctx *c, int *choice_fp32, int *choice_fp64)
         c->shape[prec] = cands[besti];
         c->tuned[prec] = 1;
     }
-    auto code = [](const gf_ctx::PassShape &sh) { return sh.variant == 1 ? sh.warps : (sh.variant == 2 ? 64 : 0); };
+    auto code = [](const gf_ctx::PassShape &sh) {
+        return sh.variant == 1 ? sh.warps : (sh.variant == 2 ? 64 : (sh.variant == 3 ? 100 : 0));
+    };
     if (choice_fp32) *choice_fp32 = c->mixed ? code(c->shape[0]) : -1;
     if (choice_fp64) *choice_fp64 = code(c->shape[1]);
     return GF_OK;
 }
 
-// Set the parity-pass launch shape by hand: variant 0 (one warp per tile) or 1 (pipelined with
-// `warps` = 2, 4 or 8 warps per block).
+// Set the parity-pass launch shape by hand: variant 0 (one warp per tile), 1 (pipelined with
+// `warps` = 2, 4 or 8 warps per block), 2 (FP32 direct capped at 64 registers) or 3 (register
+// prefetch, persistent).
 int gf_set_pass_shape(gf_ctx *c, int real, int variant, int warps)
 {
     clear_error();
-    if (!c || !valid_real(real) || variant < 0 || variant > 2 || (warps != 2 && warps != 4 && warps != 8) ||
-        (variant == 1 && c->gauge == GF_COULOMB) || (variant == 1 && real == GF_FP32 && c->refine) ||
+    if (!c || !valid_real(real) || variant < 0 || variant > 3 || (warps != 2 && warps != 4 && warps != 8) ||
+        (variant != 0 && variant != 2 && c->gauge == GF_COULOMB) || (variant == 1 && real == GF_FP32 && c->refine) ||
         (variant == 2 && real == GF_FP64)) {
-        set_error("invalid pass shape (Coulomb and refine-FP32 passes are direct; the 64-register pass is FP32)");
+        set_error("invalid pass shape (Coulomb passes are direct or 64-register; refine-FP32 passes are not "
+                  "pipelined; the 64-register pass is FP32)");
         return GF_ERR_INVALID;
     }
     c->shape[real].variant = variant;

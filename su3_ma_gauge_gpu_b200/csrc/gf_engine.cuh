@@ -14,7 +14,7 @@
 
 namespace gfb {
 
-enum InstState : int { ST_FP32 = 0, ST_FP64 = 1, ST_DONE = 2, ST_SWITCH = 3 };
+enum InstState : int { ST_FP32 = 0, ST_FP64 = 1, ST_DONE = 2, ST_SWITCH = 3, ST_FOLD = 4 };
 
 struct InstDesc {
     Geom g;
@@ -26,7 +26,7 @@ struct InstDesc {
     double2 *f64;         // packed FP64 field
     double2 *t64;         // Coulomb: the slice's original temporal links (6 double2 planes), else null
     int next;             // Coulomb: instance of timeslice t+1 of the same lattice, else -1
-    float2 *w;            // refine mode: accumulated gauge transformation, 9 float2 planes, else null
+    float2 *w;            // refine mode: accumulated gauge transformation, columns 0, 1 (6 float2 planes), else null
 };
 
 struct EngineDev {
@@ -39,6 +39,8 @@ struct EngineDev {
     double *quality;      // per instance: functional, theta
     double *partials;     // per quality block: 2 doubles
     unsigned int *tickets;// per instance
+    double *best32;       // per instance: smallest FP32 theta of the current gf_fix
+    int *stall;           // per instance: checks in a row without beating 0.98 * best32
 };
 
 // index of the instance whose range [begin[i], begin[i+1]) holds x (ranges ascending)
@@ -84,25 +86,118 @@ __global__ void __launch_bounds__(128, MINB) k_batched_pass(EngineDev e, int64_t
                                                                                pi, d.w);
 }
 
+// Persistent variant with register prefetch: every warp walks a strided list of 8-site tiles and
+// issues the loads of tile t+1 (its lane's two links, and the W column in refine mode) into
+// registers before it computes tile t, so each warp keeps a tile's worth of loads in flight
+// through its arithmetic and shuffles.  Same site update as k_batched_pass; not for COULOMB.
+template <typename R>
+struct TileRegs {
+    int inst;        // -1: nothing to do
+    int64_t h, s, sd;
+    R up[12], dn[12];
+    float2 w[3];
+};
+
+template <typename R, bool SITE_W>
+__device__ __forceinline__ void fetch_tile_regs(const EngineDev &e, int64_t tile, int parity, int want_state,
+                                                TileRegs<R> &t)
+{
+    t.inst = -1;
+    const int i = find_instance(e.inst, e.ninst, tile, [](const InstDesc &d) { return d.warp_begin; });
+    if (e.state[i] != want_state) return;
+    const InstDesc &d = e.inst[i];
+    const int lane = threadIdx.x & 31, mu = lane >> 3;
+    t.inst = i;
+    t.h = (tile - d.warp_begin) * 8 + (lane & 7);
+    int32_t c[4];
+    site_coords(d.g, t.h, parity, c);
+    t.s = t.h + (parity ? d.g.Vh : 0);
+    t.sd = neighbour_down(d.g, c, mu);
+    const PackedField<R> f = packed_of<R>(d);
+    f.load12(t.s, mu, t.up);
+    f.load12(t.sd, mu, t.dn);
+    if (SITE_W) {
+        const int k = mu & 1;
+#pragma unroll
+        for (int r = 0; r < 3; r++) t.w[r] = d.w[(int64_t)(k * 3 + r) * d.g.V + t.s];
+    }
+}
+
+template <typename R, int GAUGE, int ALGO, bool SITE_W>
+__global__ void __launch_bounds__(128) k_batched_pass_rp(EngineDev e, int64_t total_warps, int parity, AlgoParams p,
+                                                         int want_state)
+{
+    static_assert(GAUGE != COULOMB, "Coulomb slices use k_batched_pass");
+    const int mu = (threadIdx.x & 31) >> 3;
+    const int64_t stride = (int64_t)gridDim.x * 4;
+    int64_t tile = (int64_t)blockIdx.x * 4 + (threadIdx.x >> 5);
+    TileRegs<R> cur;
+    cur.inst = -1;
+    if (tile < total_warps) fetch_tile_regs<R, SITE_W>(e, tile, parity, want_state, cur);
+    for (; tile < total_warps; tile += stride) {
+        TileRegs<R> nxt;
+        nxt.inst = -1;
+        if (tile + stride < total_warps) fetch_tile_regs<R, SITE_W>(e, tile + stride, parity, want_state, nxt);
+        if (cur.inst >= 0) {
+            const InstDesc &d = e.inst[cur.inst];
+            Link<R> up, dn;
+            unpack12(up, cur.up);
+            reconstruct(up);
+            unpack12(dn, cur.dn);
+            reconstruct(dn);
+            Rng<R> rng;
+            if (ALGO == ALG_SA || ALGO == ALG_SR || ALGO == ALG_RANDOM)
+                rng.init(ref_rng_tid(cur.h), p.seed + (uint32_t)cur.inst, p.counter);
+            Cx<R> wcol[3];
+            if (SITE_W) {
+#pragma unroll
+                for (int r = 0; r < 3; r++) wcol[r] = cx<R>((R)cur.w[r].x, (R)cur.w[r].y);
+            }
+            site_update<GAUGE, ALGO, R, SITE_W>(up, dn, mu, p, rng, &wcol);
+            const PackedField<R> f = packed_of<R>(d);
+            store_link<R>(f, cur.s, mu, up);
+            store_link<R>(f, cur.sd, mu, dn);
+            if (SITE_W && mu < 2) {
+#pragma unroll
+                for (int r = 0; r < 3; r++)
+                    d.w[(int64_t)(mu * 3 + r) * d.g.V + cur.s] = make_float2((float)wcol[r].x, (float)wcol[r].y);
+            }
+        }
+        cur = nxt;
+    }
+}
+
 // ---- refine mode: FP64 master + FP32 working copy + accumulated W --------------------------------
+// W(x) is kept as the first two columns of D = W - 1 (6 float2 planes of V): storing the
+// deviation from the identity keeps FP32 relative accuracy on the small rotations of the late
+// sweeps, when every fold resets W to 1.  The third column of W is conj(c0 x c1), which holds
+// for every SU(3) matrix; W stays in SU(3) because every factor g is (reprojection at the
+// reference's cadence removes the FP32 drift).  The sweeps only update columns 0 and 1.
 __device__ __forceinline__ void load_w_f64(const InstDesc &d, int64_t s, Link<double> &W)
 {
 #pragma unroll
-    for (int k = 0; k < 3; k++)
+    for (int k = 0; k < 2; k++)
 #pragma unroll
         for (int r = 0; r < 3; r++) {
             const float2 v = d.w[(int64_t)(k * 3 + r) * d.g.V + s];
-            W.e[r][k] = cx<double>(v.x, v.y);
+            W.e[r][k] = cx<double>((double)v.x + (r == k ? 1.0 : 0.0), v.y);
         }
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        const int j = (i + 1) % 3, k = (i + 2) % 3;
+        const Cx<double> a = cmul(W.e[j][0], W.e[k][1]), b = cmul(W.e[k][0], W.e[j][1]);
+        W.e[i][2] = cx<double>(a.x - b.x, -(a.y - b.y));
+    }
 }
 
 __device__ __forceinline__ void store_w(const InstDesc &d, int64_t s, const Link<double> &W)
 {
 #pragma unroll
-    for (int k = 0; k < 3; k++)
+    for (int k = 0; k < 2; k++)
 #pragma unroll
         for (int r = 0; r < 3; r++)
-            d.w[(int64_t)(k * 3 + r) * d.g.V + s] = make_float2((float)W.e[r][k].x, (float)W.e[r][k].y);
+            d.w[(int64_t)(k * 3 + r) * d.g.V + s] =
+                make_float2((float)(W.e[r][k].x - (r == k ? 1.0 : 0.0)), (float)W.e[r][k].y);
 }
 
 // import of a refine instance: FP64 master and FP32 working copy of the links, W = 1
@@ -211,6 +306,46 @@ __global__ void __launch_bounds__(256) k_apply_w(EngineDev e, int64_t total_link
     double r[12];
     pack12(L, r);
     packed_of<double>(d).store12(s, mu, r);  // each thread reads and writes only its own link
+}
+
+// iterative refinement (refine contexts, fold mode): every instance in ST_FOLD folds its
+// accumulated W into the FP64 master and restarts the FP32 working copy from it, so the rounding
+// of the FP32 sweeps never accumulates past one check chunk.  W is reset by k_fold_reset_w in a
+// second launch, because this one reads W(x + mu) of neighbouring sites.
+__global__ void __launch_bounds__(256) k_fold_apply(EngineDev e, int64_t total_links)
+{
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= total_links) return;
+    const int i = find_instance(e.inst, e.ninst, idx, [](const InstDesc &d) { return d.link_begin; });
+    if (e.state[i] != ST_FOLD) return;
+    const InstDesc d = e.inst[i];
+    const int64_t l = idx - d.link_begin;
+    const int mu = (int)(l / d.g.V);
+    const int64_t s = l - mu * d.g.V;
+    Link<double> L;
+    apply_w_link(d, s, mu, L);
+    double r[12];
+    float f[12];
+    pack12(L, r);
+#pragma unroll
+    for (int k = 0; k < 12; k++) f[k] = (float)r[k];
+    packed_of<double>(d).store12(s, mu, r);
+    packed_of<float>(d).store12(s, mu, f);
+}
+
+__global__ void __launch_bounds__(256) k_fold_reset_w(EngineDev e, int64_t total_links)
+{
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= total_links) return;
+    const int i = find_instance(e.inst, e.ninst, idx, [](const InstDesc &d) { return d.link_begin; });
+    if (e.state[i] != ST_FOLD) return;
+    const InstDesc d = e.inst[i];
+    const int64_t l = idx - d.link_begin;
+    if (l >= d.g.V) return;  // one thread per site
+#pragma unroll
+    for (int k = 0; k < 2; k++)
+#pragma unroll
+        for (int r = 0; r < 3; r++) d.w[(int64_t)(k * 3 + r) * d.g.V + l] = make_float2(0.f, 0.f);  // D = 0
 }
 
 // export of a refine instance still in FP32: W U64 W^dagger on the fly
@@ -360,7 +495,8 @@ constexpr size_t staged_smem_bytes(int warps)
 }
 
 // Quality of every instance in state want_state, with the state transitions of the check:
-//  ST_FP32 -> ST_SWITCH when theta < switch_theta (mixed runs), ST_FP64 -> ST_DONE when
+//  ST_FP32 -> ST_SWITCH when theta < switch_theta (mixed runs) or when theta has stopped
+//  falling in FP32 (stall_checks), ST_FP64 -> ST_DONE when
 //  theta < precision; either -> ST_DONE when the sweep budget is spent.  chunk_sweeps is added
 //  to the instance's sweep count first.  Per-instance tickets make the last block of each
 //  instance reduce that instance's partials in block order (deterministic).
@@ -372,7 +508,26 @@ struct CheckParams {
     double precision;
     int stop_max;
     int transitions;      // 0: only measure
+    int stall_checks;     // ST_FP32 -> ST_SWITCH also after this many checks without progress
+    int fold;             // refine contexts: ST_FP32 -> ST_FOLD (not ST_SWITCH) below switch_theta
 };
+
+// progress of an instance's theta: a new best when it falls below 0.98 x the best so far;
+// returns the number of checks in a row without one
+__device__ __forceinline__ int track_progress(EngineDev e, int i, double tn)
+{
+    double best = e.best32[i];
+    int stall = e.stall[i];
+    if (tn < 0.98 * best) {
+        best = tn;
+        stall = 0;
+    } else {
+        stall++;
+    }
+    e.best32[i] = best;
+    e.stall[i] = stall;
+    return stall;
+}
 
 template <int GAUGE, typename R, int NT = 256>
 __global__ void __launch_bounds__(NT) k_batched_quality(EngineDev e, int64_t total_blocks, CheckParams cp)
@@ -417,7 +572,28 @@ __global__ void __launch_bounds__(NT) k_batched_quality(EngineDev e, int64_t tot
             e.sweeps[i] = sw;
             if (cp.want_state == ST_FP64) e.sweeps64[i] += cp.chunk_sweeps;
             int st = cp.want_state;
-            if (st == ST_FP32 && cp.switch_theta > 0 && tn < cp.switch_theta) st = ST_SWITCH;
+            if (cp.want_state == ST_FP32) {
+                if (sw == cp.chunk_sweeps) {  // first check of this gf_fix
+                    e.best32[i] = 1e300;
+                    e.stall[i] = 0;
+                }
+                if (cp.switch_theta > 0 && tn < cp.switch_theta)
+                    st = cp.fold ? ST_FOLD : ST_SWITCH;
+                else if (track_progress(e, i, tn) >= cp.stall_checks && cp.stall_checks > 0 && cp.switch_theta > 0)
+                    st = ST_SWITCH;  // FP32 rounding floor: no 2% gain within stall_checks checks
+            } else if (cp.want_state == ST_FOLD) {
+                // theta of the FP64 master right after a fold: done, keep refining in FP32, or
+                // (folds no longer gaining 2% within stall_checks folds) polish with FP64 sweeps
+                if (tn < cp.precision) {
+                    st = ST_DONE;
+                    e.storage[i] = 1;
+                } else if (track_progress(e, i, tn) >= cp.stall_checks && cp.stall_checks > 0) {
+                    st = ST_FP64;
+                    e.storage[i] = 1;
+                } else {
+                    st = ST_FP32;
+                }
+            }
             if (st == ST_FP64 && tn < cp.precision) st = ST_DONE;
             if (sw >= cp.max_sweeps) st = ST_DONE;
             e.state[i] = st;

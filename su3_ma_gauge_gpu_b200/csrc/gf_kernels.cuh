@@ -53,7 +53,7 @@ __device__ __forceinline__ void parity_pass_warp(const F &Fup, const F &Fdw, con
     if (ALGO == ALG_SA || ALGO == ALG_SR || ALGO == ALG_RANDOM) rng.init(ref_rng_tid(h), p.seed, p.counter);
     Cx<R> wcol[3];
     if (SITE_W) {
-        const int k = mu < 3 ? mu : 0;
+        const int k = mu & 1;  // lanes mu = 0, 1 own columns 0, 1 of W; 2, 3 re-read them
 #pragma unroll
         for (int r = 0; r < 3; r++) {
             const float2 v = Wsite[(int64_t)(k * 3 + r) * g.V + s];
@@ -62,7 +62,7 @@ __device__ __forceinline__ void parity_pass_warp(const F &Fup, const F &Fdw, con
     }
     site_update<GAUGE, ALGO, R, SITE_W>(up, dn, mu, p, rng, &wcol);
     store_link<R>(Fup, s, mu, up);
-    if (SITE_W && mu < 3) {
+    if (SITE_W && mu < 2) {
 #pragma unroll
         for (int r = 0; r < 3; r++) Wsite[(int64_t)(mu * 3 + r) * g.V + s] = make_float2((float)wcol[r].x, (float)wcol[r].y);
     }

@@ -51,6 +51,8 @@ class Schedule:
     sr_max_iter: int = 0
     sr_parameter: float = 1.7
     sr_stop_theta: float = 1e-6
+    stall_checks: int = 5  # not in the reference (no mixed precision there); 0 turns it off
+    fold: int = 1          # refine contexts: iterative refinement below switch_theta (0: FP64 sweeps)
 
     @classmethod
     def mag_app(cls, **kw) -> "Schedule":

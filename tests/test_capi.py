@@ -63,3 +63,19 @@ def test_validation_without_gpu():
     assert L.gf_quality_prefactor_gff(0) == pytest.approx(1 / 12)
     assert L.gf_quality_prefactor_gff(1) == pytest.approx(1 / 9)
     assert L.gf_quality_prefactor_a(2) == pytest.approx(1 / 3)
+
+
+def test_context_parameter_checks_without_gpu():
+    """gf_create validates its parameters before touching the device."""
+    from su3_ma_gauge_gpu_b200 import _lib
+
+    L = _lib.lib()
+    sizes = (ctypes.c_int32 * 4)(4, 4, 4, 4)
+    h = ctypes.c_void_p()
+    p = _lib.CtxParams(gauge=_lib.GF_COULOMB, ninstances=1, sizes=sizes, mixed=2, stream=None)
+    assert L.gf_create(ctypes.byref(p), ctypes.byref(h)) == _lib.GF_ERR_UNSUPPORTED
+    assert b"refine" in L.gf_last_error_string()
+    p = _lib.CtxParams(gauge=_lib.GF_LANDAU, ninstances=1, sizes=sizes, mixed=3, stream=None)
+    assert L.gf_create(ctypes.byref(p), ctypes.byref(h)) == _lib.GF_ERR_INVALID
+    p = _lib.CtxParams(gauge=_lib.GF_LANDAU, ninstances=0, sizes=sizes, mixed=0, stream=None)
+    assert L.gf_create(ctypes.byref(p), ctypes.byref(h)) == _lib.GF_ERR_INVALID

@@ -167,20 +167,24 @@ def test_fix_mixed_rough_field_reports_copy(cuda):
     assert res[True].gff == pytest.approx(res[False].gff, rel=1e-5)
 
 
-@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+@pytest.mark.parametrize("prec", ["fp32", "fp64", "refine"])
 def test_pipelined_pass_bit_identical_to_direct(cuda, prec):
-    """The cp.async-pipelined OR pass (2, 4, 8 warps per block) computes exactly what the direct
-    pass computes, on a batch of uneven lattices."""
+    """Every launch shape of the OR pass -- cp.async-pipelined (2, 4, 8 warps per block), register
+    prefetch (persistent), 64-register FP32 -- computes exactly what the direct pass computes, on a
+    batch of uneven lattices; in refine mode including the accumulated W (the export applies it)."""
     from su3_ma_gauge_gpu_b200.engine import GaugeFixer
 
     sizes = [(4, 4, 4, 4), (2, 6, 4, 8), (8, 8, 8, 8)]
     fields = [S.smooth_config(s, 0.3, 50 + i)[0] for i, s in enumerate(sizes)]
-    mixed = prec == "fp32"
+    mixed = {"fp32": True, "fp64": False, "refine": "refine"}[prec]
     outs = {}
-    shapes = [(0, 4), (1, 2), (1, 4), (1, 8)] + ([(2, 4)] if prec == "fp32" else [])
+    if prec == "refine":
+        shapes = [(0, 4), (2, 4), (3, 4)]
+    else:
+        shapes = [(0, 4), (1, 2), (1, 4), (1, 8), (3, 4)] + ([(2, 4)] if prec == "fp32" else [])
     for variant, warps in shapes:
         with GaugeFixer(sizes, mixed=mixed) as gf:
-            gf.set_pass_shape(prec, variant, warps)
+            gf.set_pass_shape("fp64" if prec == "fp64" else "fp32", variant, warps)
             for i, U in enumerate(fields):
                 gf.load(i, U)
             gf.sweeps("or", 4, 1.7)
@@ -206,7 +210,7 @@ def test_autotune_picks_a_shape(cuda):
         before = np.zeros_like(U)
         gf.store(0, before)
         c32, c64 = gf.autotune()
-        assert c32 in (0, 64, 2, 4, 8) and c64 in (0, 2, 4, 8)
+        assert c32 in (0, 64, 100, 2, 4, 8) and c64 in (0, 100, 2, 4, 8)
         after = np.zeros_like(U)
         gf.store(0, after)
         assert np.array_equal(before, after)  # tuning ran on a scratch copy
@@ -305,7 +309,8 @@ def _mag_app_temperatures(sa_steps, sa_min, sa_max, lo, hi, factor):
 
 def test_mag_app_schedule(cuda):
     """SA do-while with 5 sweeps per temperature and the slowed window, SR, then OR in mixed
-    precision, for MAG."""
+    precision, for MAG.  MAG's theta stalls near 2e-7 in FP32 (the oracle shows the same floor),
+    far above switch_theta: the stall rule moves the instance to the FP64 polish."""
     from su3_ma_gauge_gpu_b200.engine import GaugeFixer, Schedule
 
     size = (4, 4, 4, 8)
@@ -320,13 +325,33 @@ def test_mag_app_schedule(cuda):
     assert rep.sa_sweeps == 5 * len(temps)
     assert rep.sr_sweeps >= 1
     assert rep.converged and rep.theta < 1e-12
+    assert 0 < rep.or_sweeps_fp64 < rep.or_sweeps
     assert rep.gff > g0[0]  # the MAG functional increased
 
 
-def test_refine_mode_lands_on_the_fp64_maximum(cuda):
-    """Refine mode (FP64 master + FP32 working copy + accumulated W): the FP32 phase only
-    chooses a gauge transformation, applied exactly to the FP64 master, so the mixed run reaches
-    the plain-FP64 maximum to 1e-10 relative in F."""
+def test_stall_rule_off_keeps_mag_in_fp32(cuda):
+    """With stall_checks = 0 the switch waits for theta < switch_theta, which FP32 MAG never
+    reaches: the run stays in FP32 and ends at the sweep cap (the old behaviour)."""
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer, Schedule
+
+    size = (4, 4, 4, 8)
+    U, _ = S.smooth_config(size, 0.3, 90)
+    sch = Schedule(or_max_iter=600, precision=1e-12, switch_theta=1e-9, check_precision=20, reproject=20,
+                   micro_updates=0, stall_checks=0)
+    with GaugeFixer([size], gauge="mag", mixed=True) as gf:
+        gf.load(0, U)
+        rep = gf.fix(sch)[0]
+    assert rep.or_sweeps_fp64 == 0 and not rep.converged
+    assert 1e-8 < rep.theta < 1e-5
+
+
+@pytest.mark.parametrize("fold", [0, 1], ids=["fp64-polish", "iterative-refinement"])
+def test_refine_mode_lands_on_the_fp64_maximum(cuda, fold):
+    """Refine mode (FP64 master + FP32 working copy + accumulated W): the FP32 sweeps only
+    choose a gauge transformation, applied exactly to the FP64 master, so the mixed run reaches
+    the plain-FP64 maximum to 1e-10 relative in F -- with FP64 polish sweeps (fold = 0) and with
+    iterative refinement (fold = 1: FP32 sweeps folded into the master after every check, theta
+    measured on the master)."""
     from su3_ma_gauge_gpu_b200.engine import GaugeFixer
 
     size = (8, 8, 8, 8)
@@ -336,10 +361,14 @@ def test_refine_mode_lands_on_the_fp64_maximum(cuda):
         for mode in (False, "refine"):
             with GaugeFixer([size], mixed=mode) as gf:
                 gf.load(0, U)
-                res[(eps, mode)] = gf.fix(_sched(precision=1e-12, switch_theta=1e-9, check_precision=10))[0]
+                res[(eps, mode)] = gf.fix(_sched(precision=1e-12, switch_theta=1e-9, check_precision=10,
+                                                 fold=fold))[0]
         r, f = res[(eps, "refine")], res[(eps, False)]
         assert r.converged and r.theta < 1e-12
-        assert 0 < r.or_sweeps_fp64 < r.or_sweeps
+        if fold:
+            assert r.or_sweeps_fp64 < r.or_sweeps // 4  # (almost) every sweep in FP32
+        else:
+            assert 0 < r.or_sweeps_fp64 < r.or_sweeps
         assert r.gff == pytest.approx(f.gff, rel=1e-10), eps
 
 

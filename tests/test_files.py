@@ -141,7 +141,7 @@ def test_errors(cuda, tmp_path):
     (tmp_path / "vogt4").write_bytes(F.vogt_header(size, 4) + F.payload_encode(U, size, F.PLAIN))
     with pytest.raises(GaugeFixError, match="4-byte reals"):
         files.read_config(tmp_path / "vogt4", "VOGT", size, dev, reinterpret=files.DOUBLE)
-    (tmp_path / "lime").write_bytes(F.ildg_file(U, (4, 6, 4, 4), TEXT))
+    (tmp_path / "lime").write_bytes(F.ildg_file(F.random_links((4, 6, 4, 4), 1), (4, 6, 4, 4), TEXT))
     with pytest.raises(GaugeFixError, match="ildg-binary-data has"):
         files.read_config(tmp_path / "lime", "ILDG", size, dev)
     (tmp_path / "nolime").write_bytes(b"\0" * 200)
