@@ -234,9 +234,14 @@ int gf_instances(gf_ctx *ctx);
 int gf_kernel_launches(gf_ctx *ctx, long long *count);
 
 /* ---- configuration files (lattice/LinkFile.hxx, lattice/filetypes/, apps/ildg.cpp, apps/qcdstag.cpp)
- * Read a configuration into / write one from the GpuPattern array U (18 reals per link, like
- * the plugin entry points) of the given precision, on the device (on_device = 1) or in host
- * memory.  The payload is transcoded on the GPU in one pass.
+ * Read a configuration into / write one from the array U (18 reals per link, like the plugin
+ * entry points) of the given precision, on the device (on_device = 1) or in host memory, in the
+ * layout GF_LAYOUT_GPU (GpuPattern, access_pattern/GpuPattern.hxx:53-56) or GF_LAYOUT_TIMESLICE
+ * (GpuPatternTimeslice, access_pattern/GpuPatternTimeslice.hxx:57-62: the Nt timeslices one
+ * after the other, each the GpuPattern array of its {1, Nx, Ny, Nz} lattice -- what the Coulomb
+ * drivers and gf_import of a GF_COULOMB context use; the reference's readILDG_timeslice /
+ * readQCDSTAG_timeslice, apps/ildg.cpp:240-451, apps/qcdstag.cpp:123-227).  The payload is
+ * transcoded on the GPU in one pass.
  *  GF_FILE_PLAIN       StandardPattern array of file_real reals, no header (LinkFile.hxx:83-167)
  *  GF_FILE_HEADERONLY  header of (file size - payload) bytes, then PLAIN; on writing, the header
  *                      is copied from template_path (FileHeaderOnly.hxx:72-103)
@@ -253,10 +258,12 @@ int gf_kernel_launches(gf_ctx *ctx, long long *count);
 #define GF_FILE_VOGT 2
 #define GF_FILE_ILDG 3
 #define GF_FILE_QCDSTAG 4
-int gf_file_read(const char *path, int format, int file_real, const int32_t size[4], int real, void *U,
+#define GF_LAYOUT_GPU 0
+#define GF_LAYOUT_TIMESLICE 1
+int gf_file_read(const char *path, int format, int file_real, const int32_t size[4], int real, int layout, void *U,
                  int on_device, void *stream);
-int gf_file_write(const char *path, int format, int file_real, const int32_t size[4], int real, const void *U,
-                  int on_device, const char *template_path, int sa_steps, void *stream);
+int gf_file_write(const char *path, int format, int file_real, const int32_t size[4], int real, int layout,
+                  const void *U, int on_device, const char *template_path, int sa_steps, void *stream);
 
 #ifdef __cplusplus
 }

@@ -53,6 +53,27 @@ def _links_to_gpu(L: np.ndarray, size, dtype) -> np.ndarray:
     return out.reshape(-1)
 
 
+def gpu_to_timeslice(U: np.ndarray, size) -> np.ndarray:
+    """GpuPattern array -> GpuPatternTimeslice array (access_pattern/GpuPatternTimeslice.hxx:57-62:
+    slice t at offset t*72*Vs holds the GpuPattern array of the {1, Nx, Ny, Nz} lattice, whose
+    parity is that of x+y+z)."""
+    nt = size[0]
+    ssize = (1,) + tuple(size[1:])
+    vs = int(np.prod(ssize))
+    L = _links_tx(np.asarray(U), size)  # (t, x, y, z, mu, k)
+    return np.concatenate([_links_to_gpu(L[t:t + 1], ssize, np.asarray(U).dtype) for t in range(nt)]).reshape(
+        nt * 72 * vs)
+
+
+def timeslice_to_gpu(T: np.ndarray, size) -> np.ndarray:
+    nt = size[0]
+    ssize = (1,) + tuple(size[1:])
+    vs = int(np.prod(ssize))
+    T = np.asarray(T).reshape(nt, 72 * vs)
+    L = np.concatenate([_links_tx(T[t], ssize) for t in range(nt)], axis=0)
+    return _links_to_gpu(L, size, T.dtype)
+
+
 def payload_encode(U: np.ndarray, size, fmt: int, file_dtype=np.float64) -> bytes:
     """The configuration payload (no header) of format fmt."""
     L = _links_tx(np.asarray(U), size)  # (t, x, y, z, mu, k)

@@ -11,7 +11,8 @@
  *   gaugefixing/apps/ildg.cpp (readILDG / writeILDG), gaugefixing/apps/qcdstag.cpp
  *   (readQCDSTAG / writeQCDSTAG) and, compiled beside it as C, the c-lime sources those use.
  * What this file adds: extern "C" wrappers with the pattern types the reference drivers use
- * (apps/LandauGaugeFixingSU3_4D.cu:53-54,119-121), and oracle/shim/boost (boost::iequals).
+ * (apps/LandauGaugeFixingSU3_4D.cu:53-54,119-121; the Coulomb apps' GpuPatternTimeslice,
+ * apps/CoulombGaugeFixingSU3_4D.cu:57-59), and oracle/shim/boost (boost::iequals).
  */
 #define __constant__
 #include <cstdint>
@@ -22,6 +23,7 @@
 #include "lattice/LinkFile.hxx"
 #include "lattice/SiteCoord.hxx"
 #include "lattice/access_pattern/GpuPattern.hxx"
+#include "lattice/access_pattern/GpuPatternTimeslice.hxx"
 #include "lattice/access_pattern/StandardPattern.hxx"
 #include "lattice/filetypes/FileHeaderOnly.hxx"
 #include "lattice/filetypes/FilePlain.hxx"
@@ -31,11 +33,12 @@
 
 typedef StandardPattern<SiteCoord<4, NO_SPLIT>, 4, 3> RefStandard;
 typedef GpuPattern<SiteCoord<4, FULL_SPLIT>, 4, 3> RefGpu;
+typedef GpuPatternTimeslice<SiteCoord<4, FULL_SPLIT>, 4, 3> RefGpuTimeslice;  // the Coulomb apps' memory pattern
 
-template <class FT>
+template <class FT, class MP = RefGpu>
 static int load_save(const char *in, const char *out, int reinterpret, double *U, const double *Unew)
 {
-    LinkFile<FT, RefStandard, RefGpu, SiteCoord<4, FULL_SPLIT>> lf((ReinterpretReal)reinterpret);
+    LinkFile<FT, RefStandard, MP, SiteCoord<4, FULL_SPLIT>> lf((ReinterpretReal)reinterpret);
     SiteCoord<4, FULL_SPLIT> s(HOST_CONSTANTS::SIZE);
     if (!lf.load(s, in, (Real *)U)) return 1;
     if (out) {
@@ -65,6 +68,54 @@ int refio_linkfile(int format, const char *in, const char *out, int reinterpret,
     if (format == 2) rc = load_save<FileVogt>(in, out, reinterpret, U, Unew);
     std::cout.rdbuf(old);
     return rc;
+}
+
+/* the same with the memory pattern of the Coulomb apps (CoulombGaugeFixingSU3_4D.cu:57-59,132-134) */
+int refio_linkfile_timeslice(int format, const char *in, const char *out, int reinterpret, double *U,
+                             const double *Unew)
+{
+    std::ostringstream sink;
+    std::streambuf *old = std::cout.rdbuf(sink.rdbuf());
+    int rc = 3;
+    if (format == 0) rc = load_save<FilePlain, RefGpuTimeslice>(in, out, reinterpret, U, Unew);
+    if (format == 1) rc = load_save<FileHeaderOnly, RefGpuTimeslice>(in, out, reinterpret, U, Unew);
+    if (format == 2) rc = load_save<FileVogt, RefGpuTimeslice>(in, out, reinterpret, U, Unew);
+    std::cout.rdbuf(old);
+    return rc;
+}
+
+int refio_read_ildg_timeslice(const char *path, double *U)
+{
+    SiteCoord<4, FULL_SPLIT> s(HOST_CONSTANTS::SIZE);
+    const short size[4] = {(short)Nt, (short)Nx, (short)Ny, (short)Nz};
+    readILDG_timeslice(s, path, size, (Real *)U);
+    return 0;
+}
+
+int refio_write_ildg_timeslice(const char *template_path, const char *out, double *U, int steps)
+{
+    SiteCoord<4, FULL_SPLIT> s(HOST_CONSTANTS::SIZE);
+    const short size[4] = {(short)Nt, (short)Nx, (short)Ny, (short)Nz};
+    writeILDG_timeslice(s, template_path, out, size, (Real *)U, steps);
+    return 0;
+}
+
+int refio_read_qcdstag_timeslice(const char *path, double *U)
+{
+    SiteCoord<4, FULL_SPLIT> s(HOST_CONSTANTS::SIZE);
+    const short size[4] = {(short)Nt, (short)Nx, (short)Ny, (short)Nz};
+    std::ostringstream sink;
+    std::streambuf *old = std::cout.rdbuf(sink.rdbuf());
+    const bool ok = readQCDSTAG_timeslice(s, path, size, (Real *)U);
+    std::cout.rdbuf(old);
+    return ok ? 0 : 1;
+}
+
+int refio_write_qcdstag_timeslice(const char *out, double *U)
+{
+    SiteCoord<4, FULL_SPLIT> s(HOST_CONSTANTS::SIZE);
+    const short size[4] = {(short)Nt, (short)Nx, (short)Ny, (short)Nz};
+    return writeQCDSTAG_timeslice(s, out, size, (Real *)U) ? 0 : 1;
 }
 
 int refio_read_ildg(const char *path, double *U)

@@ -24,6 +24,7 @@ GF_LANDAU, GF_COULOMB, GF_MAG, GF_U1XU1 = 0, 1, 2, 3
 GF_FP32, GF_FP64 = 0, 1
 GF_MAX, GF_AVERAGE = 0, 1
 GF_FILE_PLAIN, GF_FILE_HEADERONLY, GF_FILE_VOGT, GF_FILE_ILDG, GF_FILE_QCDSTAG = 0, 1, 2, 3, 4
+GF_LAYOUT_GPU, GF_LAYOUT_TIMESLICE = 0, 1
 
 _c_int, _c_float, _c_double = ctypes.c_int, ctypes.c_float, ctypes.c_double
 _vp = ctypes.c_void_p
@@ -48,9 +49,9 @@ SIGNATURES = {
     "gf_stats_generate": (_c_int, [_vp, _vp, _vp, _dp, _dp]),
     "gf_stats_destroy": (_c_int, [_vp]),
     "gf_quality_noalloc": (_c_int, [_c_int, _c_int, _vp, _i32p, _c_int, _vp, _dp, _dp]),
-    "gf_file_read": (_c_int, [ctypes.c_char_p, _c_int, _c_int, _i32p, _c_int, _vp, _c_int, _vp]),
-    "gf_file_write": (_c_int, [ctypes.c_char_p, _c_int, _c_int, _i32p, _c_int, _vp, _c_int, ctypes.c_char_p, _c_int,
-                               _vp]),
+    "gf_file_read": (_c_int, [ctypes.c_char_p, _c_int, _c_int, _i32p, _c_int, _c_int, _vp, _c_int, _vp]),
+    "gf_file_write": (_c_int, [ctypes.c_char_p, _c_int, _c_int, _i32p, _c_int, _c_int, _vp, _c_int, ctypes.c_char_p,
+                               _c_int, _vp]),
 }
 
 

@@ -55,9 +55,26 @@ __device__ __forceinline__ int64_t file_link_offset(const Geom &g, const int32_t
     return ((int64_t)mu * Nt * Nx * Ny * Nz + lf) * 18;  // QCDSTAG: file direction kept
 }
 
-// one thread per link (s, mu): file buffer -> GpuPattern (all 18 reals)
+// Memory side: GpuPattern (GF_LAYOUT_GPU, access_pattern/GpuPattern.hxx:53-56) or
+// GpuPatternTimeslice (GF_LAYOUT_TIMESLICE, access_pattern/GpuPatternTimeslice.hxx:57-62: slice t
+// is the GpuPattern array of the {1, Nx, Ny, Nz} lattice, spatial parity, at offset t * 72 Vs).
+// Returns the offset of real 0 of link (coords c, mu) and the stride between its 18 reals.
+__device__ __forceinline__ int64_t memory_link_offset(const Geom &g, const Geom &gs, const int32_t c[4], int mu,
+                                                      int64_t s, int layout, int64_t &stride)
+{
+    if (layout == GF_LAYOUT_GPU) {
+        stride = g.V;
+        return (int64_t)mu * 18 * g.V + s;
+    }
+    const int32_t cs[4] = {0, c[1], c[2], c[3]};
+    stride = gs.V;
+    return (int64_t)c[0] * 72 * gs.V + (int64_t)mu * 18 * gs.V + site_index(gs, cs);
+}
+
+// one thread per link (s, mu): file buffer -> memory layout (all 18 reals)
 template <typename Rf, typename R>
-__global__ void __launch_bounds__(256) k_file_to_gpu(const Rf *file, Geom g, int order, int swap, R *U)
+__global__ void __launch_bounds__(256) k_file_to_gpu(const Rf *file, Geom g, Geom gs, int order, int swap,
+                                                     int layout, R *U)
 {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= 4 * g.V) return;
@@ -67,17 +84,19 @@ __global__ void __launch_bounds__(256) k_file_to_gpu(const Rf *file, Geom g, int
     int32_t c[4];
     site_coords(g, s - (parity ? g.Vh : 0), parity, c);
     const Rf *src = file + file_link_offset(g, c, mu, order);
-    R *dst = U + (int64_t)mu * 18 * g.V + s;
+    int64_t stride;
+    R *dst = U + memory_link_offset(g, gs, c, mu, s, layout, stride);
 #pragma unroll
     for (int k = 0; k < 18; k++) {
         double v = (double)src[k];
         if (sizeof(Rf) == 8 && swap) v = bswap_f64(v);
-        dst[k * g.V] = (R)v;
+        dst[k * stride] = (R)v;
     }
 }
 
 template <typename R, typename Rf>
-__global__ void __launch_bounds__(256) k_gpu_to_file(const R *U, Geom g, int order, int swap, Rf *file)
+__global__ void __launch_bounds__(256) k_gpu_to_file(const R *U, Geom g, Geom gs, int order, int swap, int layout,
+                                                     Rf *file)
 {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (idx >= 4 * g.V) return;
@@ -87,10 +106,11 @@ __global__ void __launch_bounds__(256) k_gpu_to_file(const R *U, Geom g, int ord
     int32_t c[4];
     site_coords(g, s - (parity ? g.Vh : 0), parity, c);
     Rf *dst = file + file_link_offset(g, c, mu, order);
-    const R *src = U + (int64_t)mu * 18 * g.V + s;
+    int64_t stride;
+    const R *src = U + memory_link_offset(g, gs, c, mu, s, layout, stride);
 #pragma unroll
     for (int k = 0; k < 18; k++) {
-        double v = (double)src[k * g.V];
+        double v = (double)src[k * stride];
         if (sizeof(Rf) == 8 && swap) v = bswap_f64(v);
         dst[k] = (Rf)v;
     }
@@ -196,25 +216,38 @@ struct DevBuf {
 };
 
 template <typename Rf>
-static int transcode_in(const void *dfile, const Geom &g, int order, int swap, int real, void *dU, cudaStream_t st)
+static int transcode_in(const void *dfile, const Geom &g, const Geom &gs, int order, int swap, int layout, int real,
+                        void *dU, cudaStream_t st)
 {
     const unsigned blocks = (unsigned)((4 * g.V + 255) / 256);
     if (real == GF_FP64)
-        k_file_to_gpu<Rf, double><<<blocks, 256, 0, st>>>((const Rf *)dfile, g, order, swap, (double *)dU);
+        k_file_to_gpu<Rf, double><<<blocks, 256, 0, st>>>((const Rf *)dfile, g, gs, order, swap, layout, (double *)dU);
     else
-        k_file_to_gpu<Rf, float><<<blocks, 256, 0, st>>>((const Rf *)dfile, g, order, swap, (float *)dU);
+        k_file_to_gpu<Rf, float><<<blocks, 256, 0, st>>>((const Rf *)dfile, g, gs, order, swap, layout, (float *)dU);
     return launch_status("file transcode");
 }
 
 template <typename Rf>
-static int transcode_out(const void *dU, const Geom &g, int order, int swap, int real, void *dfile, cudaStream_t st)
+static int transcode_out(const void *dU, const Geom &g, const Geom &gs, int order, int swap, int layout, int real,
+                         void *dfile, cudaStream_t st)
 {
     const unsigned blocks = (unsigned)((4 * g.V + 255) / 256);
     if (real == GF_FP64)
-        k_gpu_to_file<double, Rf><<<blocks, 256, 0, st>>>((const double *)dU, g, order, swap, (Rf *)dfile);
+        k_gpu_to_file<double, Rf><<<blocks, 256, 0, st>>>((const double *)dU, g, gs, order, swap, layout, (Rf *)dfile);
     else
-        k_gpu_to_file<float, Rf><<<blocks, 256, 0, st>>>((const float *)dU, g, order, swap, (Rf *)dfile);
+        k_gpu_to_file<float, Rf><<<blocks, 256, 0, st>>>((const float *)dU, g, gs, order, swap, layout, (Rf *)dfile);
     return launch_status("file transcode");
+}
+
+// geometry of one timeslice {1, Nx, Ny, Nz} (only used for GF_LAYOUT_TIMESLICE)
+static int slice_geom(const int32_t size[4], int layout, Geom &gs)
+{
+    if (layout != GF_LAYOUT_TIMESLICE) {
+        gs = Geom{};
+        return GF_OK;
+    }
+    const int32_t ss[4] = {1, size[1], size[2], size[3]};
+    return make_geom(ss, GF_COULOMB, true, gs);
 }
 
 }  // namespace gfb
@@ -223,18 +256,18 @@ using namespace gfb;
 
 extern "C" {
 
-int gf_file_read(const char *path, int format, int file_real, const int32_t size[4], int real, void *U, int on_device,
-                 void *stream)
+int gf_file_read(const char *path, int format, int file_real, const int32_t size[4], int real, int layout, void *U,
+                 int on_device, void *stream)
 {
     clear_error();
     if (!path || !U || !valid_real(real) || !valid_real(file_real) || format < GF_FILE_PLAIN ||
-        format > GF_FILE_QCDSTAG) {
+        format > GF_FILE_QCDSTAG || (layout != GF_LAYOUT_GPU && layout != GF_LAYOUT_TIMESLICE)) {
         set_error("invalid argument to gf_file_read");
         return GF_ERR_INVALID;
     }
-    Geom g;
+    Geom g, gs;
     int st = make_geom(size, GF_LANDAU, false, g);
-    if (st) return st;
+    if (st || (st = slice_geom(size, layout, gs))) return st;
     const bool dbl = (format == GF_FILE_ILDG || format == GF_FILE_QCDSTAG) ? true : file_real == GF_FP64;
     const size_t es = dbl ? 8 : 4;
     const size_t payload = (size_t)g.V * 72 * es;
@@ -325,24 +358,25 @@ int gf_file_read(const char *path, int format, int file_real, const int32_t size
     }
     const int order = format == GF_FILE_ILDG ? ORD_ILDG : (format == GF_FILE_QCDSTAG ? ORD_QCDSTAG : ORD_STANDARD);
     const int swap = format == GF_FILE_ILDG;
-    st = dbl ? transcode_in<double>(dfile.p, g, order, swap, real, dU, s) : transcode_in<float>(dfile.p, g, order, swap, real, dU, s);
+    st = dbl ? transcode_in<double>(dfile.p, g, gs, order, swap, layout, real, dU, s)
+             : transcode_in<float>(dfile.p, g, gs, order, swap, layout, real, dU, s);
     if (st) return st;
     if (!on_device && (st = cuda_status(cudaMemcpyAsync(U, dU, ubytes, cudaMemcpyDeviceToHost, s), "D2H"))) return st;
     return cuda_status(cudaStreamSynchronize(s), "file read sync");
 }
 
-int gf_file_write(const char *path, int format, int file_real, const int32_t size[4], int real, const void *U,
-                  int on_device, const char *template_path, int sa_steps, void *stream)
+int gf_file_write(const char *path, int format, int file_real, const int32_t size[4], int real, int layout,
+                  const void *U, int on_device, const char *template_path, int sa_steps, void *stream)
 {
     clear_error();
     if (!path || !U || !valid_real(real) || !valid_real(file_real) || format < GF_FILE_PLAIN ||
-        format > GF_FILE_QCDSTAG) {
+        format > GF_FILE_QCDSTAG || (layout != GF_LAYOUT_GPU && layout != GF_LAYOUT_TIMESLICE)) {
         set_error("invalid argument to gf_file_write");
         return GF_ERR_INVALID;
     }
-    Geom g;
+    Geom g, gs;
     int st = make_geom(size, GF_LANDAU, false, g);
-    if (st) return st;
+    if (st || (st = slice_geom(size, layout, gs))) return st;
     const bool dbl = (format == GF_FILE_ILDG || format == GF_FILE_QCDSTAG) ? true : file_real == GF_FP64;
     const size_t es = dbl ? 8 : 4;
     const size_t payload = (size_t)g.V * 72 * es;
@@ -358,8 +392,8 @@ int gf_file_write(const char *path, int format, int file_real, const int32_t siz
     if ((st = cuda_status(cudaMalloc(&dfile.p, payload), "cudaMalloc"))) return st;
     const int order = format == GF_FILE_ILDG ? ORD_ILDG : (format == GF_FILE_QCDSTAG ? ORD_QCDSTAG : ORD_STANDARD);
     const int swap = format == GF_FILE_ILDG;
-    st = dbl ? transcode_out<double>(dU, g, order, swap, real, dfile.p, s)
-             : transcode_out<float>(dU, g, order, swap, real, dfile.p, s);
+    st = dbl ? transcode_out<double>(dU, g, gs, order, swap, layout, real, dfile.p, s)
+             : transcode_out<float>(dU, g, gs, order, swap, layout, real, dfile.p, s);
     if (st) return st;
     PinnedBuf host;
     if ((st = cuda_status(cudaHostAlloc(&host.p, payload, cudaHostAllocDefault), "cudaHostAlloc"))) return st;

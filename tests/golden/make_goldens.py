@@ -9,7 +9,8 @@ Every entry is the SHA-256 of what the reference code returns for a seeded input
     (oracle/_ref/libref_pin_f64.so: GaugeFixingSubgroupStep.hxx + algorithms/*Update.hxx);
   * setHot, projectSU3 and the per-site gauge quality, FP64;
   * the bytes of the configuration files the reference's LinkFile / writeILDG / writeQCDSTAG
-    write, and the array its readers load (oracle/_ref/libref_io.so).
+    write, and the array its readers load, with the GpuPattern memory pattern and with the
+    Coulomb apps' GpuPatternTimeslice one (oracle/_ref/libref_io.so).
 tests/test_golden.py recomputes the same with the oracle (no reference needed) and compares, so
 the oracle stays pinned on machines without the reference tree.
 """
@@ -130,6 +131,26 @@ def main():
         h["file/qcdstag/read"] = sha(got)
         io.refio_write_qcdstag(str(d / "out").encode(), Ub.ctypes.data_as(dp))
         h["file/qcdstag/write"] = sha((d / "out").read_bytes())
+        # the Coulomb apps' memory pattern (GpuPatternTimeslice): reads and writes
+        Tb = F.gpu_to_timeslice(Ub, FILE_SIZE)
+        (d / "in").write_bytes(F.payload_encode(Ua, FILE_SIZE, F.PLAIN))
+        got = np.zeros(V72)
+        assert io.refio_linkfile_timeslice(0, str(d / "in").encode(), str(d / "out").encode(), 1,
+                                           got.ctypes.data_as(dp), Tb.ctypes.data_as(dp)) == 0
+        h["file/timeslice/plain/read"] = sha(got)
+        h["file/timeslice/plain/write"] = sha((d / "out").read_bytes())
+        (d / "in").write_bytes(F.ildg_file(Ua, FILE_SIZE, FILE_TEXT))
+        got = np.zeros(V72)
+        io.refio_read_ildg_timeslice(str(d / "in").encode(), got.ctypes.data_as(dp))
+        h["file/timeslice/ildg/read"] = sha(got)
+        io.refio_write_ildg_timeslice(str(d / "in").encode(), str(d / "out").encode(), Tb.ctypes.data_as(dp), 17)
+        h["file/timeslice/ildg/write"] = sha((d / "out").read_bytes())
+        (d / "in").write_bytes(F.payload_encode(Ua, FILE_SIZE, F.QCDSTAG))
+        got = np.zeros(V72)
+        assert io.refio_read_qcdstag_timeslice(str(d / "in").encode(), got.ctypes.data_as(dp)) == 0
+        h["file/timeslice/qcdstag/read"] = sha(got)
+        io.refio_write_qcdstag_timeslice(str(d / "out").encode(), Tb.ctypes.data_as(dp))
+        h["file/timeslice/qcdstag/write"] = sha((d / "out").read_bytes())
     OUT.write_text(json.dumps(h, indent=1, sort_keys=True) + "\n")
     print(f"wrote {len(h)} hashes to {OUT}")
 

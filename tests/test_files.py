@@ -102,6 +102,50 @@ def test_write_matches_oracle(cuda, tmp_path, size, fname):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("fname", ["plain", "headeronly", "ildg", "qcdstag"])
+def test_timeslice_layout(cuda, tmp_path, fname):
+    """GpuPatternTimeslice (the Coulomb apps' memory pattern): read, write back, and the array
+    feeds a Coulomb context directly."""
+    torch = cuda
+    fmt, size = FORMATS[fname], (4, 6, 4, 2)
+    U = F.random_links(size, 51)
+    path = tmp_path / "cfg"
+    path.write_bytes(_file_bytes(U, size, fmt))
+    dev = torch.empty(U.size, dtype=torch.float64, device="cuda")
+    files.read_config(path, fmt, size, dev, "double", files.DOUBLE, layout="timeslice")
+    assert np.array_equal(dev.cpu().numpy(), F.gpu_to_timeslice(U, size))
+    out = tmp_path / "out"
+    files.write_config(out, fmt, size, dev, "double", files.DOUBLE, template=path, sa_steps=3, layout="timeslice")
+    want = F.ildg_rewrite(path.read_bytes(), U, size, 3) if fmt == F.ILDG else path.read_bytes()
+    assert out.read_bytes() == want
+
+
+@pytest.mark.gpu
+def test_coulomb_context_from_timeslice_file(cuda, tmp_path):
+    """A configuration file read in the timeslice layout goes straight into a Coulomb context."""
+    from su3_ma_gauge_gpu_b200 import synthetic as S
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer
+
+    torch = cuda
+    size = (4, 4, 4, 6)
+    U, _ = S.smooth_config(size, 0.3, 7)
+    path = tmp_path / "cfg.lime"
+    path.write_bytes(F.ildg_file(U, size, TEXT))
+    T = torch.empty(U.size, dtype=torch.float64, device="cuda")
+    files.readILDG_timeslice(size, path, T)
+    with GaugeFixer([size], gauge="coulomb", mixed=False) as gf:
+        gf.load(0, T)
+        g, a = gf.quality()
+    import _oracle as O
+
+    Ts = F.gpu_to_timeslice(U, size)
+    Vs = int(np.prod(size[1:]))
+    for t in range(size[0]):
+        gq, aq = O.quality(Ts[t * 72 * Vs:(t + 1) * 72 * Vs].copy(), (1,) + size[1:], O.COULOMB)
+        assert g[t] == pytest.approx(gq, rel=1e-12) and a[t] == pytest.approx(aq, rel=1e-10)
+
+
+@pytest.mark.gpu
 def test_linkfile_and_app_readers(cuda, tmp_path):
     """The reference-named entry points: LinkFile.load/save keeps the header; ILDG / QCDSTAG."""
     torch = cuda

@@ -69,3 +69,11 @@ def test_file_formats_hash():
     tmpl = F.ildg_file(Ua, S, G.FILE_TEXT)
     assert sha(F.ildg_rewrite(tmpl, Ub, S, 17)) == GOLD["file/ildg/write"]
     assert sha(F.payload_encode(Ub, S, F.QCDSTAG)) == GOLD["file/qcdstag/write"]
+    # GpuPatternTimeslice (Coulomb apps): same files, the arrays in timeslice order
+    Ta = F.gpu_to_timeslice(Ua, S)
+    for fmt in ("plain", "ildg", "qcdstag"):
+        assert sha(Ta) == GOLD[f"file/timeslice/{fmt}/read"], fmt
+    assert GOLD["file/timeslice/plain/write"] == GOLD["file/plain_f64/write"]
+    assert GOLD["file/timeslice/ildg/write"] == GOLD["file/ildg/write"]
+    assert GOLD["file/timeslice/qcdstag/write"] == GOLD["file/qcdstag/write"]
+    assert np.array_equal(F.timeslice_to_gpu(Ta, S), Ua)
