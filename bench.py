@@ -41,7 +41,22 @@ METRIC = "Gsite-updates/s & HBM GB/s; time-to-theta<1e-12 mixed/batched vs plain
 UNIT = "Gsite-updates/s"
 SIZE = (32, 32, 32, 32)
 EPS = 0.3
-BYTES_PER_SITE_UPDATE = {"fp32": 768, "fp64": 1536}  # 8 links x 12 reals x (read + write)
+# 8 links x 12 reals x (read + write); the refine-mode FP32 pass also reads and writes the two
+# tracked columns of the site's W - 1 (6 complex floats = 48 B each way)
+BYTES_PER_SITE_UPDATE = {"fp32": 768, "fp64": 1536, "fp32_refine": 768 + 96}
+
+
+def pass_kernel_name(code: int, real: str, refine: bool) -> str:
+    """The OR-pass kernel an autotuner choice stands for (gf_autotune's output codes)."""
+    r = "float" if real == "fp32" else "double"
+    w = ", W" if refine and real == "fp32" else ""
+    if code == 100:
+        return f"k_batched_pass_rp<{r}, LANDAU, OR{w}> (register prefetch, persistent)"
+    if code == 64:
+        return f"k_batched_pass<{r}, LANDAU, OR{w}> (64 registers)"
+    if code in (2, 4, 8):
+        return f"k_batched_pass_staged<{r}, LANDAU, OR, {code} warps>"
+    return f"k_batched_pass<{r}, LANDAU, OR{w}>"
 
 
 def env_rank():
@@ -509,25 +524,27 @@ def main():
     Vh = V // 2
     n64 = rep.or_sweeps_fp64
     n32 = sweeps - n64
-    kern = {"fp32": {"ms_per_launch": t32, "gbs": Vh * BYTES_PER_SITE_UPDATE["fp32"] / (t32 * 1e-3) / 1e9,
-                     "launches_per_step": 2 * n32}}
+    b32 = BYTES_PER_SITE_UPDATE["fp32_refine" if args.mixed == "refine" else "fp32"]
+    kern = {"fp32": {"ms_per_launch": t32, "gbs": Vh * b32 / (t32 * 1e-3) / 1e9, "launches_per_step": 2 * n32,
+                     "bytes_per_site_update": b32}}
     if t64 is not None:
         kern["fp64"] = {"ms_per_launch": t64, "gbs": Vh * BYTES_PER_SITE_UPDATE["fp64"] / (t64 * 1e-3) / 1e9,
-                        "launches_per_step": 2 * n64}
+                        "launches_per_step": 2 * n64, "bytes_per_site_update": BYTES_PER_SITE_UPDATE["fp64"]}
     dom = max(kern, key=lambda k: kern[k]["ms_per_launch"] * kern[k]["launches_per_step"])
     traffic = None
     tfile = ROOT / "profiles" / "or_pass_traffic.json"
     if tfile.exists():
         try:
-            traffic = json.loads(tfile.read_text()).get(dom)
+            tkey = "fp32_refine" if dom == "fp32" and args.mixed == "refine" else dom
+            traffic = json.loads(tfile.read_text()).get(tkey)
         except Exception:
             traffic = None
     roofline = {"bound": "hbm", "achieved": kern[dom]["gbs"], "peak": peak, "unit": "GB/s",
                 "frac": kern[dom]["gbs"] / peak, "traffic": traffic,
-                "kernel": (f"k_batched_pass{'_staged' if tuned[0 if dom == 'fp32' else 1] else ''}"
-                           f"<{'float' if dom == 'fp32' else 'double'}, LANDAU, OR> (one parity pass)"),
+                "kernel": pass_kernel_name(tuned[0 if dom == "fp32" else 1], dom, args.mixed == "refine")
+                + " (one parity pass)",
                 "launch_shape": {"fp32": tuned[0], "fp64": tuned[1]},
-                "algorithmic_bytes_per_launch": Vh * BYTES_PER_SITE_UPDATE[dom], "peak_kind": peak_kind,
+                "algorithmic_bytes_per_launch": Vh * kern[dom]["bytes_per_site_update"], "peak_kind": peak_kind,
                 "per_precision": kern}
 
     cpu = None

@@ -183,6 +183,13 @@ typedef struct gf_schedule {
                               working copy restarts from the master, and theta is measured on the
                               master in FP64; FP64 sweeps only if folds stop gaining (stall_checks).
                               0 = switch to FP64 sweeps at switch_theta */
+    int trace_checks;      /* > 0: record up to this many OR checks per instance (gf_trace); the
+                              reference prints the same line at every check */
+    double fold_exit;      /* fold mode: once the master's theta after a fold is below fold_exit x
+                              precision, the instance finishes with FP64 sweeps.  The FP32 working
+                              copy leaves a rounding-noise floor of about 1e-12 in the master's
+                              theta that only FP64 sweeps remove (they do so within ~20 sweeps);
+                              0: fold until theta < precision or the folds stall */
 } gf_schedule;
 
 typedef struct gf_report {
@@ -230,6 +237,12 @@ int gf_autotune(gf_ctx *ctx, int *choice_fp32, int *choice_fp64);
 int gf_set_pass_shape(gf_ctx *ctx, int real, int variant, int warps);
 /* Number of instances (lattices, or timeslices for GF_COULOMB). */
 int gf_instances(gf_ctx *ctx);
+/* The OR checks of the last gf_fix with schedule.trace_checks > 0: for instance `instance`, up to
+ * max_entries entries of 4 doubles {OR sweeps so far, precision of the check (0 = FP32 working
+ * copy, 1 = FP64, 4 = FP64 master right after an iterative-refinement fold), functional, theta};
+ * *n = entries available (at most trace_checks: the first ones are kept); call with max_entries =
+ * 0 to size the buffer. */
+int gf_trace(gf_ctx *ctx, int instance, double *out, int max_entries, int *n);
 /* Number of kernels this context has launched so far (each node of a replayed graph counts). */
 int gf_kernel_launches(gf_ctx *ctx, long long *count);
 

@@ -75,7 +75,7 @@ class Schedule(ctypes.Structure):
                 ("sa_repeat", ctypes.c_int), ("sa_slow_lo", ctypes.c_double), ("sa_slow_hi", ctypes.c_double),
                 ("sa_slow_factor", ctypes.c_float), ("sr_max_iter", ctypes.c_int), ("sr_parameter", ctypes.c_float),
                 ("sr_stop_theta", ctypes.c_double), ("stall_checks", ctypes.c_int),
-                ("fold", ctypes.c_int)]
+                ("fold", ctypes.c_int), ("trace_checks", ctypes.c_int), ("fold_exit", ctypes.c_double)]
 
 
 class Report(ctypes.Structure):
@@ -97,6 +97,7 @@ SIGNATURES.update({
     "gf_set_storage": (_c_int, [_vp, _c_int]),
     "gf_fix": (_c_int, [_vp, ctypes.POINTER(Schedule), ctypes.POINTER(Report)]),
     "gf_kernel_launches": (_c_int, [_vp, ctypes.POINTER(ctypes.c_longlong)]),
+    "gf_trace": (_c_int, [_vp, _c_int, _dp, _c_int, ctypes.POINTER(_c_int)]),
     "gf_autotune": (_c_int, [_vp, ctypes.POINTER(_c_int), ctypes.POINTER(_c_int)]),
     "gf_set_pass_shape": (_c_int, [_vp, _c_int, _c_int, _c_int]),
     "gf_instances": (_c_int, [_vp]),

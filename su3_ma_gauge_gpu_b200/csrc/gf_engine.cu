@@ -34,6 +34,9 @@ struct gf_ctx {
     double2 *f64 = nullptr;
     int *d_state = nullptr, *d_sweeps = nullptr, *d_sweeps64 = nullptr, *d_storage = nullptr;
     double *d_quality = nullptr, *d_partials = nullptr;
+    double *d_trace = nullptr;    // OR check trace (gf_schedule.trace_checks), else null
+    int *d_ntrace = nullptr;
+    int trace_cap = 0;
     unsigned int *d_tickets = nullptr;
     int *h_state = nullptr;       // pinned (state, then storage: 2 * ninst)
     double *h_quality = nullptr;  // pinned
@@ -72,6 +75,9 @@ struct gf_ctx {
         e.partials = d_partials;
         e.tickets = d_tickets;
         e.best32 = d_quality + 2 * ninst;
+        e.trace = d_trace;
+        e.ntrace = d_ntrace;
+        e.trace_cap = trace_cap;
         e.stall = d_state + 4 * ninst;
         return e;
     }
@@ -303,9 +309,10 @@ int enqueue_or_chunk(gf_ctx *c, int nsweeps, float omega, bool reproject, const 
             // iterative refinement: instances now in ST_FOLD fold W into the FP64 master, restart
             // the working copy, and are checked on the master (their sweeps are already counted)
             const unsigned blocks = grid_for(c->total_links, 256);
+            k_reunitarise_w<<<blocks, 256, 0, c->stream>>>(c->dev(), c->total_links, ST_FOLD);
             k_fold_apply<<<blocks, 256, 0, c->stream>>>(c->dev(), c->total_links);
             k_fold_reset_w<<<blocks, 256, 0, c->stream>>>(c->dev(), c->total_links);
-            c->launches += 2;
+            c->launches += 3;
             if ((st = launch_status("fold"))) return st;
             CheckParams cf = cp;
             cf.want_state = ST_FOLD;
@@ -481,6 +488,8 @@ int gf_destroy(gf_ctx *c)
     cudaFree(c->d_inst);
     cudaFree(c->d_state);
     cudaFree(c->d_quality);
+    cudaFree(c->d_trace);
+    cudaFree(c->d_ntrace);
     cudaFree(c->d_partials);
     cudaFree(c->d_tickets);
     cudaFree(c->staging);
@@ -612,6 +621,37 @@ int gf_export(gf_ctx *c, int lat, int real, void *U, int on_host)
     return cuda_status(cudaStreamSynchronize(c->stream), "export sync");
 }
 
+}  // extern "C"
+
+namespace {
+
+// which precisions the instances sweep in, from the host copy of the states
+void present_states(const gf_ctx *c, bool &has32, bool &has64)
+{
+    has32 = has64 = false;
+    for (int i = 0; i < c->ninst; i++) {
+        has32 |= c->h_state[i] == ST_FP32;
+        has64 |= c->h_state[i] == ST_FP64;
+    }
+}
+
+int sweeps_on(gf_ctx *c, int algo, int nsweeps, float param, int seed, int rng_counter, bool has32, bool has64)
+{
+    int st = GF_OK;
+    uint32_t ctr = (uint32_t)rng_counter;
+    for (int k = 0; k < nsweeps && !st; k++) {
+        // the reference takes a fresh Philox counter per launch (PhiloxWrapper::getNextCounter)
+        if (c->mixed && has32) st = launch_sweep(c, algo, ST_FP32, param, (uint32_t)seed, ctr, ctr + 1);
+        if (!st && has64) st = launch_sweep(c, algo, ST_FP64, param, (uint32_t)seed, ctr, ctr + 1);
+        ctr += 2;
+    }
+    return st;
+}
+
+}  // namespace
+
+extern "C" {
+
 int gf_sweeps(gf_ctx *c, int algo, int nsweeps, float param, int seed, int rng_counter)
 {
     clear_error();
@@ -621,14 +661,11 @@ int gf_sweeps(gf_ctx *c, int algo, int nsweeps, float param, int seed, int rng_c
         set_error("invalid algorithm %d or sweep count %d", algo, nsweeps);
         return GF_ERR_INVALID;
     }
-    uint32_t ctr = (uint32_t)rng_counter;
-    for (int k = 0; k < nsweeps && !st; k++) {
-        // the reference takes a fresh Philox counter per launch (PhiloxWrapper::getNextCounter)
-        if (c->mixed) st = launch_sweep(c, algo, ST_FP32, param, (uint32_t)seed, ctr, ctr + 1);
-        if (!st) st = launch_sweep(c, algo, ST_FP64, param, (uint32_t)seed, ctr, ctr + 1);
-        ctr += 2;
-    }
-    return st;
+    // launch only the precisions some instance is sweeping in (an empty pass still costs a grid)
+    if ((st = sync_states(c))) return st;
+    bool has32, has64;
+    present_states(c, has32, has64);
+    return sweeps_on(c, algo, nsweeps, param, seed, rng_counter, has32, has64);
 }
 
 int gf_reunitarize(gf_ctx *c)
@@ -702,6 +739,13 @@ int gf_fix(gf_ctx *c, const gf_schedule *s, gf_report *rep)
     if (s->autotune && (!c->tuned[1] || (c->mixed && !c->tuned[0])) && (st = gf_autotune(c, nullptr, nullptr)))
         return st;
     uint32_t ctr = s->rng_counter;
+    // the precisions the instances sweep in before the OR phase (set by gf_import)
+    if ((st = sync_states(c))) return st;
+    bool pre32, pre64;
+    present_states(c, pre32, pre64);
+    auto gf_sweeps = [&](gf_ctx *cc, int algo, int n, float param, int seed, int counter) {
+        return sweeps_on(cc, algo, n, param, seed, counter, pre32, pre64);
+    };
     // random gauge transformation of every instance (apps/LandauGaugeFixingSU3_4D.cu:192-196)
     if (s->random_trafo) {
         if ((st = gf_sweeps(c, ALG_RANDOM, 1, 0.f, (int)s->seed, (int)ctr))) return st;
@@ -779,12 +823,35 @@ int gf_fix(gf_ctx *c, const gf_schedule *s, gf_report *rep)
     base.stop_max = 0;
     base.stall_checks = s->stall_checks;
     base.fold = c->refine ? s->fold : 0;
+    base.fold_exit = s->fold_exit > 0 ? s->fold_exit : 0.0;
     {
         std::vector<int> zeros(2 * c->ninst, 0);
         if ((st = cuda_status(cudaMemcpyAsync(c->d_sweeps, zeros.data(), sizeof(int) * 2 * c->ninst,
                                               cudaMemcpyHostToDevice, c->stream), "sweeps reset")))
             return st;
     }
+    // optional check trace: (re)allocated for this run's capacity, or switched off
+    if (s->trace_checks > 0 && s->trace_checks != c->trace_cap) {
+        cudaFree(c->d_trace);
+        cudaFree(c->d_ntrace);
+        c->d_trace = nullptr;
+        c->d_ntrace = nullptr;
+        c->trace_cap = 0;
+        if ((st = cuda_status(cudaMalloc(&c->d_trace, sizeof(double) * 4 * (size_t)s->trace_checks * c->ninst),
+                              "cudaMalloc trace")) ||
+            (st = cuda_status(cudaMalloc(&c->d_ntrace, sizeof(int) * c->ninst), "cudaMalloc trace")))
+            return st;
+        c->trace_cap = s->trace_checks;
+    } else if (s->trace_checks <= 0 && c->trace_cap) {
+        cudaFree(c->d_trace);
+        cudaFree(c->d_ntrace);
+        c->d_trace = nullptr;
+        c->d_ntrace = nullptr;
+        c->trace_cap = 0;
+    }
+    if (c->trace_cap && (st = cuda_status(cudaMemsetAsync(c->d_ntrace, 0, sizeof(int) * c->ninst, c->stream),
+                                          "trace reset")))
+        return st;
     if ((st = sync_states(c))) return st;
     const int C = s->check_precision;
     struct Variant {
@@ -1017,6 +1084,34 @@ int gf_set_pass_shape(gf_ctx *c, int real, int variant, int warps)
 }
 
 int gf_instances(gf_ctx *c) { return c ? c->ninst : 0; }
+
+int gf_trace(gf_ctx *c, int instance, double *out, int max_entries, int *n)
+{
+    clear_error();
+    int st = check_ctx(c);
+    if (st) return st;
+    if (instance < 0 || instance >= c->ninst || max_entries < 0 || (max_entries > 0 && !out) || !n) {
+        set_error("invalid argument to gf_trace");
+        return GF_ERR_INVALID;
+    }
+    *n = 0;
+    if (!c->trace_cap) return GF_OK;
+    int cnt = 0;
+    if ((st = cuda_status(cudaMemcpyAsync(&cnt, c->d_ntrace + instance, sizeof(int), cudaMemcpyDeviceToHost,
+                                          c->stream), "trace count")) ||
+        (st = cuda_status(cudaStreamSynchronize(c->stream), "sync")))
+        return st;
+    *n = std::min(cnt, c->trace_cap);
+    const int m = std::min(*n, max_entries);
+    if (m > 0) {
+        if ((st = cuda_status(cudaMemcpyAsync(out, c->d_trace + (size_t)instance * c->trace_cap * 4,
+                                              sizeof(double) * 4 * m, cudaMemcpyDeviceToHost, c->stream),
+                              "trace copy")))
+            return st;
+        return cuda_status(cudaStreamSynchronize(c->stream), "sync");
+    }
+    return GF_OK;
+}
 
 int gf_kernel_launches(gf_ctx *c, long long *count)
 {

@@ -41,6 +41,9 @@ struct EngineDev {
     unsigned int *tickets;// per instance
     double *best32;       // per instance: smallest FP32 theta of the current gf_fix
     int *stall;           // per instance: checks in a row without beating 0.98 * best32
+    double *trace;        // optional: trace_cap entries of 4 doubles per instance, else null
+    int *ntrace;          // per instance: checks recorded (may exceed trace_cap)
+    int trace_cap;
 };
 
 // index of the instance whose range [begin[i], begin[i+1]) holds x (ranges ascending)
@@ -246,8 +249,10 @@ __global__ void __launch_bounds__(256) k_reunitarise_w(EngineDev e, int64_t tota
     store_w(d, l, W);
 }
 
-// U64_mu(x) <- W(x) U64_mu(x) W(x+mu)^dagger, reunitarised, in FP64 (W reunitarised first)
-__device__ __forceinline__ void apply_w_link(const InstDesc &d, int64_t s, int mu, Link<double> &L)
+// U64_mu(x) <- W(x) U64_mu(x) W(x+mu)^dagger, reunitarised, in FP64 (W reunitarised first unless
+// the caller has projected every W of the instance already)
+__device__ __forceinline__ void apply_w_link(const InstDesc &d, int64_t s, int mu, Link<double> &L,
+                                             bool project_w = true)
 {
     const int parity = s >= d.g.Vh;
     int32_t c[4];
@@ -256,8 +261,10 @@ __device__ __forceinline__ void apply_w_link(const InstDesc &d, int64_t s, int m
     Link<double> W, Wf, T;
     load_w_f64(d, s, W);
     load_w_f64(d, sf, Wf);
-    project_rows(W);
-    project_rows(Wf);
+    if (project_w) {
+        project_rows(W);
+        project_rows(Wf);
+    }
     load_link_f64<double>(packed_of<double>(d), s, mu, T);
     Link<double> M;
 #pragma unroll
@@ -310,8 +317,9 @@ __global__ void __launch_bounds__(256) k_apply_w(EngineDev e, int64_t total_link
 
 // iterative refinement (refine contexts, fold mode): every instance in ST_FOLD folds its
 // accumulated W into the FP64 master and restarts the FP32 working copy from it, so the rounding
-// of the FP32 sweeps never accumulates past one check chunk.  W is reset by k_fold_reset_w in a
-// second launch, because this one reads W(x + mu) of neighbouring sites.
+// of the FP32 sweeps never accumulates past one check chunk.  k_reunitarise_w projects each W
+// once before (instead of twice per link here); W is reset by k_fold_reset_w in a separate
+// launch, because this one reads W(x + mu) of neighbouring sites.
 __global__ void __launch_bounds__(256) k_fold_apply(EngineDev e, int64_t total_links)
 {
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -323,7 +331,7 @@ __global__ void __launch_bounds__(256) k_fold_apply(EngineDev e, int64_t total_l
     const int mu = (int)(l / d.g.V);
     const int64_t s = l - mu * d.g.V;
     Link<double> L;
-    apply_w_link(d, s, mu, L);
+    apply_w_link(d, s, mu, L, false);  // k_reunitarise_w has projected every W of the instance
     double r[12];
     float f[12];
     pack12(L, r);
@@ -510,6 +518,7 @@ struct CheckParams {
     int transitions;      // 0: only measure
     int stall_checks;     // ST_FP32 -> ST_SWITCH also after this many checks without progress
     int fold;             // refine contexts: ST_FP32 -> ST_FOLD (not ST_SWITCH) below switch_theta
+    double fold_exit;     // ST_FOLD -> ST_FP64 once theta < fold_exit * precision (0: off)
 };
 
 // progress of an instance's theta: a new best when it falls below 0.98 x the best so far;
@@ -570,6 +579,16 @@ __global__ void __launch_bounds__(NT) k_batched_quality(EngineDev e, int64_t tot
         if (cp.transitions) {
             const int sw = e.sweeps[i] + cp.chunk_sweeps;
             e.sweeps[i] = sw;
+            if (e.trace) {
+                const int k = e.ntrace[i]++;
+                if (k < e.trace_cap) {
+                    double *t = e.trace + ((int64_t)i * e.trace_cap + k) * 4;
+                    t[0] = sw;
+                    t[1] = cp.want_state;
+                    t[2] = gn;
+                    t[3] = tn;
+                }
+            }
             if (cp.want_state == ST_FP64) e.sweeps64[i] += cp.chunk_sweeps;
             int st = cp.want_state;
             if (cp.want_state == ST_FP32) {
@@ -582,12 +601,15 @@ __global__ void __launch_bounds__(NT) k_batched_quality(EngineDev e, int64_t tot
                 else if (track_progress(e, i, tn) >= cp.stall_checks && cp.stall_checks > 0 && cp.switch_theta > 0)
                     st = ST_SWITCH;  // FP32 rounding floor: no 2% gain within stall_checks checks
             } else if (cp.want_state == ST_FOLD) {
-                // theta of the FP64 master right after a fold: done, keep refining in FP32, or
-                // (folds no longer gaining 2% within stall_checks folds) polish with FP64 sweeps
+                // theta of the FP64 master right after a fold: done; or within fold_exit of the
+                // target, where the FP32 rounding noise (~1e-12) is a visible part of it, or with
+                // the folds no longer gaining 2% within stall_checks folds: polish with FP64
+                // sweeps; else keep refining in FP32
                 if (tn < cp.precision) {
                     st = ST_DONE;
                     e.storage[i] = 1;
-                } else if (track_progress(e, i, tn) >= cp.stall_checks && cp.stall_checks > 0) {
+                } else if (tn < cp.fold_exit * cp.precision ||
+                           (track_progress(e, i, tn) >= cp.stall_checks && cp.stall_checks > 0)) {
                     st = ST_FP64;
                     e.storage[i] = 1;
                 } else {

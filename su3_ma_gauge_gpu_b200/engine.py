@@ -53,6 +53,8 @@ class Schedule:
     sr_stop_theta: float = 1e-6
     stall_checks: int = 5  # not in the reference (no mixed precision there); 0 turns it off
     fold: int = 1          # refine contexts: iterative refinement below switch_theta (0: FP64 sweeps)
+    trace_checks: int = 0  # > 0: keep that many OR checks per instance for GaugeFixer.trace()
+    fold_exit: float = 4.0  # fold mode: FP64 sweeps once the master's theta < fold_exit * precision
 
     @classmethod
     def mag_app(cls, **kw) -> "Schedule":
@@ -163,6 +165,18 @@ class GaugeFixer:
         check(lib().gf_fix(self._h, ctypes.byref(s), reps), "gf_fix")
         return [Report(r.gff, r.theta, r.or_sweeps, r.or_sweeps_fp64, r.sa_sweeps, bool(r.converged), r.chunks,
                        r.sr_sweeps) for r in reps]
+
+    def trace(self, i: int) -> np.ndarray:
+        """OR checks of instance i in the last fix with trace_checks > 0: rows (sweeps, precision
+        of the check: 0 FP32 / 1 FP64 / 4 FP64 master after a fold, functional, theta)."""
+        n = ctypes.c_int()
+        check(lib().gf_trace(self._h, i, None, 0, ctypes.byref(n)), "gf_trace")
+        m = n.value
+        buf = np.zeros(4 * max(m, 1))
+        if m:
+            check(lib().gf_trace(self._h, i, buf.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), m, ctypes.byref(n)),
+                  "gf_trace")
+        return buf[:4 * min(m, n.value)].reshape(-1, 4)
 
     def autotune(self):
         """Time the OR-pass launch shapes and keep the fastest; returns (fp32, fp64) choices."""
