@@ -52,6 +52,10 @@ def pass_kernel_name(code: int, real: str, refine: bool) -> str:
     w = ", W" if refine and real == "fp32" else ""
     if code == 100:
         return f"k_batched_pass_rp<{r}, LANDAU, OR{w}> (register prefetch, persistent)"
+    if code == 32:
+        return f"k_batched_pass_site<{r}, LANDAU, OR{w}> (one thread per site)"
+    if code == 33:
+        return f"k_batched_pass_site_staged<LANDAU, OR{w}> (one thread per site, cp.async pipelined)"
     if code == 64:
         return f"k_batched_pass<{r}, LANDAU, OR{w}> (64 registers)"
     if code in (2, 4, 8):
@@ -187,8 +191,8 @@ def run_profile_target(nsweeps: int, mode: str = "fast"):
     `nsweeps` OR sweeps per launch shape in FP32, then the same in FP64.
     mode "fast": FP32 storage; shapes direct, pipelined (4 warps per block) -- 8 * nsweeps
     parity-pass launches.  mode "refine": FP64 master + FP32 working copy with W; FP32 shapes
-    direct, 64-register, register prefetch, then FP64 direct, pipelined (4), register prefetch --
-    12 * nsweeps parity-pass launches."""
+    direct, 64-register, register prefetch, thread per site (plain, pipelined), then FP64 direct,
+    pipelined (4), register prefetch -- 16 * nsweeps parity-pass launches."""
     import torch
 
     from su3_ma_gauge_gpu_b200 import synthetic as S
@@ -197,7 +201,7 @@ def run_profile_target(nsweeps: int, mode: str = "fast"):
     U, _ = S.smooth_config(SIZE, EPS, 1234, device="cuda")
     torch.cuda.empty_cache()  # keep the device footprint of the profiled launches small
     dU = torch.from_numpy(U).cuda()
-    shapes = {"fp32": (0, 1), "fp64": (0, 1)} if mode == "fast" else {"fp32": (0, 2, 3), "fp64": (0, 1, 3)}
+    shapes = {"fp32": (0, 1), "fp64": (0, 1)} if mode == "fast" else {"fp32": (0, 2, 3, 4, 5), "fp64": (0, 1, 3)}
     with GaugeFixer([SIZE], mixed=True if mode == "fast" else "refine") as gf:
         gf.load(0, dU)
         for real in ("fp32", "fp64"):

@@ -227,13 +227,16 @@ int gf_set_storage(gf_ctx *ctx, int real);
 int gf_fix(gf_ctx *ctx, const gf_schedule *schedule, gf_report *reports);
 /* Autotuner: times the candidate launch shapes of the OR parity pass (one warp per 8-site tile;
  * the same capped at 64 registers (FP32); persistent with the next tile prefetched into
- * registers; pipelined with cp.async prefetch and 2, 4 or 8 warps per block) on a scratch copy
- * of the field (and of W in refine contexts) and keeps the fastest per precision.  Outputs: 0 =
- * direct, 64 = direct with 64 registers, 100 = register prefetch, 2/4/8 = warps per block of the
- * pipelined pass (-1: precision not used). */
+ * registers; FP32 with one thread per site; pipelined with cp.async prefetch and 2, 4 or 8 warps
+ * per block) on a scratch copy of the field (and of W in refine contexts) and keeps the fastest
+ * per precision.  Outputs: 0 = direct, 64 = direct with 64 registers, 100 = register prefetch,
+ * 32 = thread per site, 33 = thread per site pipelined with cp.async, 2/4/8 = warps per block of
+ * the pipelined pass (-1: precision not used). */
 int gf_autotune(gf_ctx *ctx, int *choice_fp32, int *choice_fp64);
 /* Fix the launch shape instead: variant 0 (direct), 1 (pipelined, warps = 2, 4 or 8), 2 (FP32
- * direct capped at 64 registers) or 3 (register prefetch).  GF_COULOMB: 0 or 2; refine FP32: not 1. */
+ * direct capped at 64 registers), 3 (register prefetch), 4 (FP32, one thread per site) or 5 (FP32,
+ * one thread per site pipelined; OR, the other rules run as 4).  GF_COULOMB: 0 or 2; refine FP32:
+ * not 1. */
 int gf_set_pass_shape(gf_ctx *ctx, int real, int variant, int warps);
 /* Number of instances (lattices, or timeslices for GF_COULOMB). */
 int gf_instances(gf_ctx *ctx);

@@ -348,11 +348,12 @@ __device__ __forceinline__ void left_mult_dcolumn(Cx<R> (&col)[3], const R g[4],
     col[J] = cx<R>(col[J].x + (q0.x + q1.x), col[J].y + (q0.y + q1.y));
 }
 
-template <int GAUGE, int ALGO, int I, int J, typename R, bool SITE_W = false>
-__device__ __forceinline__ void subgroup_step(Link<R> &up, Link<R> &dn, int mu, const AlgoParams &p, Rng<R> &rng,
-                                              Cx<R> (*wcol)[3] = nullptr)
+// Contribution of direction mu (its up link U_mu(x) and down link U_mu(x-mu)) to the subgroup
+// quaternion w of the site, before the sum over mu (GaugeFixingSubgroupStep.hxx:99-237 Landau and
+// Coulomb, :238-353 U1xU1, :354-589 MAG; MAG's factor 2 and square root follow the sum).
+template <int GAUGE, int I, int J, typename R>
+__device__ __forceinline__ void subgroup_contrib(const Link<R> &up, const Link<R> &dn, int mu, R v[4])
 {
-    R w[4];
     if (GAUGE == MAG) {
         const Cx<R> u00 = up.e[I][I], u01 = up.e[I][J], u10 = up.e[J][I], u11 = up.e[J][J];
         const Cx<R> d00 = dn.e[I][I], d01 = dn.e[I][J], d10 = dn.e[J][I], d11 = dn.e[J][J];
@@ -363,29 +364,42 @@ __device__ __forceinline__ void subgroup_step(Link<R> &up, Link<R> &dn, int mu, 
         const R cuy = (u00.y * u10.x - u00.x * u10.y) - (u01.y * u11.x - u01.x * u11.y);
         const R cdx = (d00.x * d01.x + d00.y * d01.y) - (d10.x * d11.x + d10.y * d11.y);
         const R cdy = (d00.x * d01.y - d00.y * d01.x) - (d10.x * d11.y - d10.y * d11.x);
-        w[0] = site_sum(Du + Dd);
-        w[1] = site_sum(cuy + cdy);
-        w[2] = site_sum(cux + cdx);
-        w[1] *= (R)2.;  // the factor 2 of GaugeFixingSubgroupStep.hxx:535-536
-        w[2] *= (R)2.;
-        w[3] = 0;
-        w[0] = w[0] + sq(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+        v[0] = Du + Dd;
+        v[1] = cuy + cdy;
+        v[2] = cux + cdx;
+        v[3] = 0;
     } else {
         R qu[4], qd[4];
         subq<I, J>(up, qu);
         subq<I, J>(dn, qd);
         const bool skip = (GAUGE == COULOMB) && (mu == 0);  // Coulomb: mu = 0 not in the sum
         if (GAUGE == U1XU1) {
-            w[0] = site_sum(qu[0] + qd[0]);
-            w[1] = 0;
-            w[2] = 0;
-            w[3] = site_sum(qd[3] - qu[3]);
+            v[0] = qu[0] + qd[0];
+            v[1] = 0;
+            v[2] = 0;
+            v[3] = qd[3] - qu[3];
         } else {
-            w[0] = site_sum(skip ? (R)0 : qu[0] + qd[0]);
-            w[1] = site_sum(skip ? (R)0 : qd[1] - qu[1]);
-            w[2] = site_sum(skip ? (R)0 : qd[2] - qu[2]);
-            w[3] = site_sum(skip ? (R)0 : qd[3] - qu[3]);
+            v[0] = skip ? (R)0 : qu[0] + qd[0];
+            v[1] = skip ? (R)0 : qd[1] - qu[1];
+            v[2] = skip ? (R)0 : qd[2] - qu[2];
+            v[3] = skip ? (R)0 : qd[3] - qu[3];
         }
+    }
+}
+
+// From the summed quaternion to the update g (in place): MAG's factor 2 and square root, the
+// update rule, and the U1xU1 / MAG renormalisation.
+template <int GAUGE, int ALGO, typename R>
+__device__ __forceinline__ void subgroup_finish(R w[4], const AlgoParams &p, Rng<R> &rng)
+{
+    if (GAUGE == MAG) {
+        w[1] *= (R)2.;  // the factor 2 of GaugeFixingSubgroupStep.hxx:535-536
+        w[2] *= (R)2.;
+        w[3] = 0;
+        w[0] = w[0] + sq(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+    } else if (GAUGE == U1XU1) {
+        w[1] = 0;
+        w[2] = 0;
     }
     apply_algo<ALGO>(w, p, rng);
     if (GAUGE == U1XU1) {
@@ -401,10 +415,51 @@ __device__ __forceinline__ void subgroup_step(Link<R> &up, Link<R> &dn, int mu, 
         w[1] *= n;
         w[2] *= n;
     }
+}
+
+template <int GAUGE, int ALGO, int I, int J, typename R, bool SITE_W = false>
+__device__ __forceinline__ void subgroup_step(Link<R> &up, Link<R> &dn, int mu, const AlgoParams &p, Rng<R> &rng,
+                                              Cx<R> (*wcol)[3] = nullptr)
+{
+    R v[4], w[4];
+    subgroup_contrib<GAUGE, I, J>(up, dn, mu, v);
+    w[0] = site_sum(v[0]);
+    w[1] = (GAUGE == U1XU1) ? (R)0 : site_sum(v[1]);
+    w[2] = (GAUGE == U1XU1) ? (R)0 : site_sum(v[2]);
+    w[3] = (GAUGE == MAG) ? (R)0 : site_sum(v[3]);
+    subgroup_finish<GAUGE, ALGO>(w, p, rng);
     left_mult<I, J>(up, w);
     const R h[4] = {w[0], -w[1], -w[2], -w[3]};
     right_mult<I, J>(dn, h);
     if (SITE_W) left_mult_dcolumn<I, J>(*wcol, w, mu & 1);
+}
+
+// One thread per site: the same subgroup step with all 8 links of the site in the thread.  The
+// sum over mu is taken in the order of the 4-lane butterfly, (v0 + v1) + (v2 + v3), so both
+// layouts do the same arithmetic (the compiler may still contract a product differently in the
+// two kernels).  With SITE_W the thread applies g to both tracked columns of D = W - 1.
+template <int GAUGE, int ALGO, int I, int J, typename R, bool SITE_W = false>
+__device__ __forceinline__ void subgroup_step_site(Link<R> (&up)[4], Link<R> (&dn)[4], const AlgoParams &p,
+                                                   Rng<R> &rng, Cx<R> (*wcols)[2][3] = nullptr)
+{
+    R v[4][4], w[4];
+#pragma unroll
+    for (int mu = 0; mu < 4; mu++) subgroup_contrib<GAUGE, I, J>(up[mu], dn[mu], mu, v[mu]);
+#pragma unroll
+    for (int k = 0; k < 4; k++) w[k] = (v[0][k] + v[1][k]) + (v[2][k] + v[3][k]);
+    if (GAUGE == U1XU1) w[1] = w[2] = 0;
+    if (GAUGE == MAG) w[3] = 0;
+    subgroup_finish<GAUGE, ALGO>(w, p, rng);
+    const R h[4] = {w[0], -w[1], -w[2], -w[3]};
+#pragma unroll
+    for (int mu = 0; mu < 4; mu++) {
+        left_mult<I, J>(up[mu], w);
+        right_mult<I, J>(dn[mu], h);
+    }
+    if (SITE_W) {
+        left_mult_dcolumn<I, J>((*wcols)[0], w, 0);
+        left_mult_dcolumn<I, J>((*wcols)[1], w, 1);
+    }
 }
 
 // the three subgroups in the reference order (0,2), (1,2), (0,1) (SU3::perSubgroup, SU3.hxx:762-771);
@@ -416,6 +471,15 @@ __device__ __forceinline__ void site_update(Link<R> &up, Link<R> &dn, int mu, co
     subgroup_step<GAUGE, ALGO, 0, 2, R, SITE_W>(up, dn, mu, p, rng, wcol);
     subgroup_step<GAUGE, ALGO, 1, 2, R, SITE_W>(up, dn, mu, p, rng, wcol);
     subgroup_step<GAUGE, ALGO, 0, 1, R, SITE_W>(up, dn, mu, p, rng, wcol);
+}
+
+template <int GAUGE, int ALGO, typename R, bool SITE_W = false>
+__device__ __forceinline__ void site_update_thread(Link<R> (&up)[4], Link<R> (&dn)[4], const AlgoParams &p,
+                                                   Rng<R> &rng, Cx<R> (*wcols)[2][3] = nullptr)
+{
+    subgroup_step_site<GAUGE, ALGO, 0, 2, R, SITE_W>(up, dn, p, rng, wcols);
+    subgroup_step_site<GAUGE, ALGO, 1, 2, R, SITE_W>(up, dn, p, rng, wcols);
+    subgroup_step_site<GAUGE, ALGO, 0, 1, R, SITE_W>(up, dn, p, rng, wcols);
 }
 
 // ---- lattice geometry -----------------------------------------------------------------------

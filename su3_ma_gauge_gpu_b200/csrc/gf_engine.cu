@@ -141,9 +141,48 @@ int launch_rp(const gf_ctx *c, const EngineDev &e, const PassArgs &a, int blocks
     return launch_status("batched parity pass (register prefetch)");
 }
 
+template <int GAUGE, int ALGO, bool SITE_W>
+int launch_site_staged(const gf_ctx *c, const EngineDev &e, const PassArgs &a, int blocks_per_sm)
+{
+    const size_t smem = SiteStage<SITE_W>::bytes;
+    auto kern = k_batched_pass_site_staged<GAUGE, ALGO, SITE_W>;
+    static int occ_cached = 0;  // also marks the opt-in to more than 48 KB of dynamic shared memory
+    if (occ_cached == 0) {
+        int st = cuda_status(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                             "cudaFuncSetAttribute");
+        if (st) return st;
+        int o = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, 128, smem) != cudaSuccess || o < 1) o = 1;
+        occ_cached = o;
+    }
+    const int occ = blocks_per_sm > 0 ? blocks_per_sm : occ_cached;
+    const int64_t need = (a.c->total_warps * 8 + 127) / 128;
+    const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)c->num_sms * occ));
+    kern<<<blocks, 128, smem, a.c->stream>>>(e, a.c->total_warps, a.parity, a.p, a.want_state);
+    return launch_status("batched parity pass (thread per site, pipelined)");
+}
+
 template <typename R, int GAUGE, int ALGO>
 int launch_pass(const gf_ctx *c, const EngineDev &e, const PassArgs &a, const gf_ctx::PassShape &sh)
 {
+    if constexpr (sizeof(R) == 4 && GAUGE != COULOMB && ALGO == ALG_OR) {
+        if (sh.variant == 5) {
+            if (c->refine) return launch_site_staged<GAUGE, ALGO, true>(c, e, a, sh.blocks_per_sm);
+            return launch_site_staged<GAUGE, ALGO, false>(c, e, a, sh.blocks_per_sm);
+        }
+    }
+    if constexpr (sizeof(R) == 4 && GAUGE != COULOMB) {
+        if (sh.variant == 4 || sh.variant == 5) {  // one thread per site (FP32); 5 = OR-only pipelined
+            const unsigned blocks = grid_for(a.c->total_warps * 8, 128);
+            if (c->refine)
+                k_batched_pass_site<R, GAUGE, ALGO, true, 2><<<blocks, 128, 0, a.c->stream>>>(
+                    e, a.c->total_warps, a.parity, a.p, a.want_state);
+            else
+                k_batched_pass_site<R, GAUGE, ALGO, false, 2><<<blocks, 128, 0, a.c->stream>>>(
+                    e, a.c->total_warps, a.parity, a.p, a.want_state);
+            return launch_status("batched parity pass (thread per site)");
+        }
+    }
     if constexpr (ALGO == ALG_OR && GAUGE != COULOMB) {
         if (sh.variant == 3) {
             if constexpr (sizeof(R) == 4) {
@@ -962,16 +1001,17 @@ int gf_autotune(gf_ctx *c, int *choice_fp32, int *choice_fp64)
     int st = check_ctx(c);
     if (st) return st;
     // direct; register prefetch (persistent); pipelined with 2, 4, 8 warps per block; (FP32 only)
-    // direct capped at 64 registers.  Coulomb passes are direct only, refine-FP32 passes (W
-    // tracking) direct, 64-register or register prefetch.
+    // direct capped at 64 registers and one thread per site (plain and pipelined).  Coulomb passes
+    // are direct only; refine-FP32 passes (W tracking) are not the 4-lane pipelined one.
     static const gf_ctx::PassShape cands64[] = {{0, 4, 0}, {3, 4, 0}, {1, 2, 0}, {1, 4, 0}, {1, 8, 0}};
-    static const gf_ctx::PassShape cands32[] = {{0, 4, 0}, {2, 4, 0}, {3, 4, 0}, {1, 2, 0}, {1, 4, 0}, {1, 8, 0}};
+    static const gf_ctx::PassShape cands32[] = {{0, 4, 0}, {2, 4, 0}, {3, 4, 0}, {4, 4, 0}, {5, 4, 0},
+                                                {1, 2, 0}, {1, 4, 0}, {1, 8, 0}};
     for (int prec = 0; prec < 2; prec++) {
         if (prec == 0 && !c->mixed) continue;
         const gf_ctx::PassShape *cands = prec == 0 ? cands32 : cands64;
-        int ncand = prec == 0 ? 6 : 5;
+        int ncand = prec == 0 ? 8 : 5;
         if (c->gauge == GF_COULOMB) ncand = 1;
-        else if (prec == 0 && c->refine) ncand = 3;
+        else if (prec == 0 && c->refine) ncand = 5;
         // scratch field, descriptors and states for this precision
         const InstDesc &last = c->h_inst.back();
         const size_t span32 = (size_t)(reinterpret_cast<const char *>(last.f32 ? last.f32 : (float4 *)nullptr) -
@@ -1056,7 +1096,12 @@ int gf_autotune(gf_ctx *c, int *choice_fp32, int *choice_fp64)
         c->tuned[prec] = 1;
     }
     auto code = [](const gf_ctx::PassShape &sh) {
-        return sh.variant == 1 ? sh.warps : (sh.variant == 2 ? 64 : (sh.variant == 3 ? 100 : 0));
+        return sh.variant == 1 ? sh.warps
+               : sh.variant == 2 ? 64
+               : sh.variant == 3 ? 100
+               : sh.variant == 4 ? 32
+               : sh.variant == 5 ? 33
+                                 : 0;
     };
     if (choice_fp32) *choice_fp32 = c->mixed ? code(c->shape[0]) : -1;
     if (choice_fp64) *choice_fp64 = code(c->shape[1]);
@@ -1064,16 +1109,17 @@ int gf_autotune(gf_ctx *c, int *choice_fp32, int *choice_fp64)
 }
 
 // Set the parity-pass launch shape by hand: variant 0 (one warp per tile), 1 (pipelined with
-// `warps` = 2, 4 or 8 warps per block), 2 (FP32 direct capped at 64 registers) or 3 (register
-// prefetch, persistent).
+// `warps` = 2, 4 or 8 warps per block), 2 (FP32 direct capped at 64 registers), 3 (register
+// prefetch, persistent), 4 (FP32, one thread per site) or 5 (the same, pipelined with cp.async;
+// OR only, other update rules fall back to variant 4).
 int gf_set_pass_shape(gf_ctx *c, int real, int variant, int warps)
 {
     clear_error();
-    if (!c || !valid_real(real) || variant < 0 || variant > 3 || (warps != 2 && warps != 4 && warps != 8) ||
+    if (!c || !valid_real(real) || variant < 0 || variant > 5 || (warps != 2 && warps != 4 && warps != 8) ||
         (variant != 0 && variant != 2 && c->gauge == GF_COULOMB) || (variant == 1 && real == GF_FP32 && c->refine) ||
-        (variant == 2 && real == GF_FP64)) {
+        ((variant == 2 || variant == 4 || variant == 5) && real == GF_FP64)) {
         set_error("invalid pass shape (Coulomb passes are direct or 64-register; refine-FP32 passes are not "
-                  "pipelined; the 64-register pass is FP32)");
+                  "pipelined; the 64-register and thread-per-site passes are FP32)");
         return GF_ERR_INVALID;
     }
     c->shape[real].variant = variant;

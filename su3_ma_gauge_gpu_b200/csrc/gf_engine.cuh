@@ -170,6 +170,73 @@ __global__ void __launch_bounds__(128) k_batched_pass_rp(EngineDev e, int64_t to
     }
 }
 
+// One thread per site: a warp updates 32 consecutive sites of a parity, each thread all 8 links
+// of its site (4 up, 4 down) in registers.  Every load and store of a plane is 32 consecutive
+// 16-byte chunks, there are no shuffles, and the subgroup quaternion and its update are computed
+// once per site instead of once per lane.  Not for COULOMB (its slices keep W in the temporal
+// planes and use the 4-lane pass).
+template <typename R, int GAUGE, int ALGO, bool SITE_W, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_batched_pass_site(EngineDev e, int64_t total_warps, int parity,
+                                                                 AlgoParams p, int want_state)
+{
+    static_assert(GAUGE != COULOMB, "Coulomb slices use k_batched_pass");
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;  // one site per thread
+    if (t >= total_warps * 8) return;
+    const int i = find_instance(e.inst, e.ninst, t >> 3, [](const InstDesc &d) { return d.warp_begin; });
+    if (e.state[i] != want_state) return;
+    const InstDesc &d = e.inst[i];
+    const int64_t h = t - d.warp_begin * 8;
+    int32_t c[4];
+    site_coords(d.g, h, parity, c);
+    const int64_t s = h + (parity ? d.g.Vh : 0);
+    const PackedField<R> f = packed_of<R>(d);
+    Link<R> up[4], dn[4];
+#pragma unroll
+    for (int mu = 0; mu < 4; mu++) {
+        R r[12];
+        f.load12(s, mu, r);
+        unpack12(up[mu], r);
+    }
+    int64_t sd[4];
+#pragma unroll
+    for (int mu = 0; mu < 4; mu++) {
+        sd[mu] = neighbour_down(d.g, c, mu);
+        R r[12];
+        f.load12(sd[mu], mu, r);
+        unpack12(dn[mu], r);
+    }
+    Cx<R> wc[2][3];
+    if (SITE_W) {
+#pragma unroll
+        for (int k = 0; k < 2; k++)
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+                const float2 v = d.w[(int64_t)(k * 3 + r) * d.g.V + s];
+                wc[k][r] = cx<R>((R)v.x, (R)v.y);
+            }
+    }
+#pragma unroll
+    for (int mu = 0; mu < 4; mu++) {
+        reconstruct(up[mu]);
+        reconstruct(dn[mu]);
+    }
+    Rng<R> rng;
+    if (ALGO == ALG_SA || ALGO == ALG_SR || ALGO == ALG_RANDOM) rng.init(ref_rng_tid(h), p.seed + (uint32_t)i, p.counter);
+    site_update_thread<GAUGE, ALGO, R, SITE_W>(up, dn, p, rng, &wc);
+#pragma unroll
+    for (int mu = 0; mu < 4; mu++) {
+        store_link<R>(f, s, mu, up[mu]);
+        store_link<R>(f, sd[mu], mu, dn[mu]);
+    }
+    if (SITE_W) {
+#pragma unroll
+        for (int k = 0; k < 2; k++)
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+                d.w[(int64_t)(k * 3 + r) * d.g.V + s] = make_float2((float)wc[k][r].x, (float)wc[k][r].y);
+    }
+}
+
 // ---- refine mode: FP64 master + FP32 working copy + accumulated W --------------------------------
 // W(x) is kept as the first two columns of D = W - 1 (6 float2 planes of V): storing the
 // deviation from the identity keeps FP32 relative accuracy on the small rotations of the late
@@ -500,6 +567,143 @@ template <typename R>
 constexpr size_t staged_smem_bytes(int warps)
 {
     return (size_t)warps * 2 * Chunks<R>::per_lane * 32 * 16;
+}
+
+// ---- one thread per site, pipelined: FP32 only ---------------------------------------------------
+// Persistent blocks of 128 threads walk 128-site tiles; every thread prefetches the 8 links of its
+// site in the next tile (24 chunks of 16 B) and, in refine mode, the 6 complex floats of its W
+// columns (3 slots of 16 B, filled by 8-byte copies) into shared memory with cp.async while it
+// updates its site of the current tile.  Slot j of a thread is at [stage][j][thread], so the
+// copies and the reads back are conflict-free and each thread only reads what it copied itself.
+template <bool SITE_W>
+struct SiteStage {
+    static constexpr int slots = 24 + (SITE_W ? 3 : 0);
+    static constexpr size_t bytes = (size_t)2 * slots * 128 * 16;
+};
+
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+// the instance and half-lattice site of global site index gsite, or -1 (inactive / past the end)
+__device__ __forceinline__ int site_of(const EngineDev &e, int64_t gsite, int64_t total_sites, int want_state,
+                                       int64_t &h)
+{
+    if (gsite >= total_sites) return -1;
+    const int i = find_instance(e.inst, e.ninst, gsite >> 3, [](const InstDesc &d) { return d.warp_begin; });
+    if (e.state[i] != want_state) return -1;
+    h = gsite - e.inst[i].warp_begin * 8;
+    return i;
+}
+
+template <bool SITE_W>
+__device__ __forceinline__ void prefetch_site(const EngineDev &e, int i, int64_t h, int parity, uint4 *stage)
+{
+    const InstDesc &d = e.inst[i];
+    int32_t c[4];
+    site_coords(d.g, h, parity, c);
+    const int64_t s = h + (parity ? d.g.Vh : 0);
+    const int t = threadIdx.x;
+#pragma unroll
+    for (int mu = 0; mu < 4; mu++) {
+        const int64_t sd = neighbour_down(d.g, c, mu);
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            cp_async16(stage + (mu * 3 + k) * 128 + t, d.f32 + (int64_t)(mu * 3 + k) * d.g.V + s);
+            cp_async16(stage + (12 + mu * 3 + k) * 128 + t, d.f32 + (int64_t)(mu * 3 + k) * d.g.V + sd);
+        }
+    }
+    if (SITE_W) {
+        float2 *ws = reinterpret_cast<float2 *>(stage + 24 * 128);
+#pragma unroll
+        for (int q = 0; q < 6; q++)  // slot q/2, half q%2
+            cp_async8(ws + ((q >> 1) * 128 + t) * 2 + (q & 1), d.w + (int64_t)q * d.g.V + s);
+    }
+}
+
+__device__ __forceinline__ void unstage_link_f32(const uint4 *stage, int first, Link<float> &L)
+{
+    float r[12];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const float4 v = reinterpret_cast<const float4 *>(stage)[(first + k) * 128 + threadIdx.x];
+        r[4 * k] = v.x;
+        r[4 * k + 1] = v.y;
+        r[4 * k + 2] = v.z;
+        r[4 * k + 3] = v.w;
+    }
+    unpack12(L, r);
+}
+
+template <int GAUGE, int ALGO, bool SITE_W>
+__global__ void __launch_bounds__(128, 2) k_batched_pass_site_staged(EngineDev e, int64_t total_warps, int parity,
+                                                                     AlgoParams p, int want_state)
+{
+    static_assert(GAUGE != COULOMB, "Coulomb slices use k_batched_pass");
+    extern __shared__ uint4 smem[];
+    constexpr int SL = SiteStage<SITE_W>::slots;
+    uint4 *stages[2] = {smem, smem + SL * 128};
+    const int64_t total_sites = total_warps * 8;
+    const int64_t stride = (int64_t)gridDim.x * 128;
+    int64_t gsite = (int64_t)blockIdx.x * 128 + threadIdx.x;
+    int64_t h = 0;
+    int inst = site_of(e, gsite, total_sites, want_state, h);
+    if (inst >= 0) prefetch_site<SITE_W>(e, inst, h, parity, stages[0]);
+    cp_async_commit();
+    int cur = 0;
+    // every thread of the block runs the same number of iterations (the tile loop is uniform)
+    for (int64_t tile0 = (int64_t)blockIdx.x * 128; tile0 < total_sites; tile0 += stride) {
+        int64_t hn = 0;
+        const int next = site_of(e, gsite + stride, total_sites, want_state, hn);
+        if (next >= 0) prefetch_site<SITE_W>(e, next, hn, parity, stages[cur ^ 1]);
+        cp_async_commit();
+        cp_async_wait<1>();
+        if (inst >= 0) {
+            const InstDesc &d = e.inst[inst];
+            int32_t c[4];
+            site_coords(d.g, h, parity, c);
+            const int64_t s = h + (parity ? d.g.Vh : 0);
+            Link<float> up[4], dn[4];
+#pragma unroll
+            for (int mu = 0; mu < 4; mu++) {
+                unstage_link_f32(stages[cur], mu * 3, up[mu]);
+                unstage_link_f32(stages[cur], 12 + mu * 3, dn[mu]);
+                reconstruct(up[mu]);
+                reconstruct(dn[mu]);
+            }
+            Cx<float> wc[2][3];
+            if (SITE_W) {
+                const float2 *ws = reinterpret_cast<const float2 *>(stages[cur] + 24 * 128);
+#pragma unroll
+                for (int q = 0; q < 6; q++) {
+                    const float2 v = ws[((q >> 1) * 128 + threadIdx.x) * 2 + (q & 1)];
+                    wc[q / 3][q % 3] = cx<float>(v.x, v.y);
+                }
+            }
+            Rng<float> rng;
+            if (ALGO == ALG_SA || ALGO == ALG_SR || ALGO == ALG_RANDOM)
+                rng.init(ref_rng_tid(h), p.seed + (uint32_t)inst, p.counter);
+            site_update_thread<GAUGE, ALGO, float, SITE_W>(up, dn, p, rng, &wc);
+            const PackedField<float> f = packed_of<float>(d);
+#pragma unroll
+            for (int mu = 0; mu < 4; mu++) {
+                store_link<float>(f, s, mu, up[mu]);
+                store_link<float>(f, neighbour_down(d.g, c, mu), mu, dn[mu]);
+            }
+            if (SITE_W) {
+#pragma unroll
+                for (int q = 0; q < 6; q++)
+                    d.w[(int64_t)q * d.g.V + s] = make_float2(wc[q / 3][q % 3].x, wc[q / 3][q % 3].y);
+            }
+        }
+        gsite += stride;
+        h = hn;
+        inst = next;
+        cur ^= 1;
+    }
+    cp_async_wait<0>();
 }
 
 // Quality of every instance in state want_state, with the state transitions of the check:
