@@ -339,6 +339,82 @@ def run_plain8(args):
                       "gsite_updates_per_s": V * rep.or_sweeps / (ms * 1e-3) / 1e9}))
 
 
+def _timed_fix(gf, loads, sched, steps, warmup, stream):
+    """warmup + steps full fixes (import, gf_fix) timed with CUDA events; returns (ms, reports)."""
+    import torch
+
+    reps = None
+    for _ in range(warmup):
+        for i, U in enumerate(loads):
+            gf.load(i, U)
+        reps = gf.fix(sched)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(max(1, steps)):
+        for i, U in enumerate(loads):
+            gf.load(i, U)
+        reps = gf.fix(sched)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / max(1, steps), reps
+
+
+def run_coulomb48(args):
+    """Coulomb gauge on a 48^3 x 16 lattice (eps = 0.3 smooth field under a Haar gauge transform):
+    all 16 timeslices fixed as independent instances in the same launches; per slice 500 SA
+    sweeps, T 1.0 -> 0.01, a microcanonical sweep after every 3rd SA sweep, then OR omega = 1.7
+    to theta < 1e-12; FP32 bulk, FP64 polish, FP64 reductions."""
+    import numpy as np
+    import torch
+
+    from su3_ma_gauge_gpu_b200 import synthetic as S
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer, Schedule
+
+    size = (16, 48, 48, 48)
+    U, _ = S.smooth_config(size, EPS, 4848, device="cuda")
+    T = torch.from_numpy(S.gpupattern_to_timeslices(U, size)).cuda()
+    stream = torch.cuda.Stream()
+    sched = Schedule(sa_steps=500, sa_min=0.01, sa_max=1.0, micro_updates=1, micro_every=3, or_max_iter=20000,
+                     precision=1e-12, switch_theta=1e-9, check_precision=args.check, reproject=100, seed=7)
+    with GaugeFixer([size], gauge="coulomb", mixed=True, stream=stream) as gf:
+        ms, reps = _timed_fix(gf, [T], sched, args.steps, args.warmup, stream)
+    V = int(np.prod(size))
+    sweeps = sum(r.or_sweeps + r.sa_sweeps for r in reps) / len(reps)
+    print(json.dumps({"workload": "coulomb48x16", "ms_per_fix": ms, "timeslices": len(reps),
+                      "all_converged": all(r.converged for r in reps), "max_theta": max(r.theta for r in reps),
+                      "or_sweeps": {"min": min(r.or_sweeps for r in reps), "max": max(r.or_sweeps for r in reps)},
+                      "sa_sweeps": reps[0].sa_sweeps, "mean_F": float(np.mean([r.gff for r in reps])),
+                      "gsite_updates_per_s": V * sweeps / (ms * 1e-3) / 1e9}))
+
+
+def run_mag48(args):
+    """Maximal Abelian gauge on a 48^4 lattice, U = exp(i*0.5*H) under a Haar gauge transform: 3000
+    SA sweeps (Philox heat-bath, geometric T 1.4 -> 0.01), then OR omega = 1.7, FP32 working copy
+    with the gauge transformation tracked (refine mode), FP64 polish to theta < 1e-12."""
+    import numpy as np
+    import torch
+
+    from su3_ma_gauge_gpu_b200 import synthetic as S
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer, Schedule
+
+    size = (48, 48, 48, 48)
+    U, _ = S.smooth_config(size, 0.5, 4849, device="cuda")
+    dU = torch.from_numpy(U).cuda()
+    del U
+    stream = torch.cuda.Stream()
+    sched = Schedule(sa_steps=3000, sa_min=0.01, sa_max=1.4, sa_geometric=1, micro_updates=0, or_max_iter=20000,
+                     precision=1e-12, switch_theta=1e-9, check_precision=args.check, reproject=100, seed=9)
+    with GaugeFixer([size], gauge="mag", mixed="refine", stream=stream) as gf:
+        ms, reps = _timed_fix(gf, [dU], sched, args.steps, args.warmup, stream)
+    r = reps[0]
+    V = int(np.prod(size))
+    print(json.dumps({"workload": "mag48", "ms_per_fix": ms, "sa_sweeps": r.sa_sweeps, "or_sweeps": r.or_sweeps,
+                      "or_sweeps_fp64": r.or_sweeps_fp64, "theta": r.theta, "F": r.gff, "converged": r.converged,
+                      "footprint_fp32_12_gb": V * 4 * 48 / 1e9,
+                      "gsite_updates_per_s": V * (r.or_sweeps + r.sa_sweeps) / (ms * 1e-3) / 1e9}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -356,9 +432,10 @@ def main():
     ap.add_argument("--mixed", default="refine", choices=["fast", "refine"],
                     help="mixed-precision mode of the headline run: fast = FP32 storage converted to FP64 at "
                          "the switch; refine = FP64 master + FP32 working copy + accumulated gauge transform")
-    ap.add_argument("--workload", default="landau32", choices=["landau32", "gribov", "plain8"],
+    ap.add_argument("--workload", default="landau32", choices=["landau32", "gribov", "plain8", "coulomb48", "mag48"],
                     help="landau32: the headline 32^4 mixed-precision fix; gribov: 64 random-gauge copies of "
-                         "uneven lattices in one batch; plain8: the 8^4 Haar-random FP64 plain fix")
+                         "uneven lattices in one batch; plain8: the 8^4 Haar-random FP64 plain fix; coulomb48: "
+                         "48^3x16 Coulomb, 16 timeslices batched, 500 SA + OR; mag48: 48^4 MAG, 3000 SA + OR")
     ap.add_argument("--profile-mode", default="fast", choices=["fast", "refine"])
     ap.add_argument("--launch-list", action="store_true",
                     help="one headline step without graphs, warm-up or clock sampling, for ncu's launch list")
@@ -380,6 +457,12 @@ def main():
         return
     if args.workload == "plain8":
         run_plain8(args)
+        return
+    if args.workload == "coulomb48":
+        run_coulomb48(args)
+        return
+    if args.workload == "mag48":
+        run_mag48(args)
         return
 
     import numpy as np

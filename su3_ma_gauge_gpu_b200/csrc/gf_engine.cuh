@@ -89,6 +89,51 @@ __global__ void __launch_bounds__(128, MINB) k_batched_pass(EngineDev e, int64_t
                                                                                pi, d.w);
 }
 
+// The descriptors and states of the first kInstCache instances, copied into shared memory once per
+// block: a persistent block looks its tile's instance up every iteration, and a chain of dependent
+// global loads there would stall every warp for an L2 round trip per tile.  Instances beyond the
+// cache are read from global memory.
+constexpr int kInstCache = 8;
+struct InstCache {
+    InstDesc d[kInstCache];
+    int state[kInstCache];
+    int n;
+};
+
+__device__ __forceinline__ void fill_inst_cache(const EngineDev &e, InstCache &ic)
+{
+    const int n = e.ninst < kInstCache ? e.ninst : kInstCache;
+    if (threadIdx.x < n) {
+        ic.d[threadIdx.x] = e.inst[threadIdx.x];
+        ic.state[threadIdx.x] = e.state[threadIdx.x];
+    }
+    if (threadIdx.x == 0) ic.n = n;
+    __syncthreads();
+}
+
+__device__ __forceinline__ const InstDesc &inst_at(const EngineDev &e, const InstCache &ic, int i)
+{
+    return i < ic.n ? ic.d[i] : e.inst[i];
+}
+
+// the instance and half-lattice site of global site index gsite, or -1 (inactive / past the end)
+__device__ __forceinline__ int site_of(const EngineDev &e, const InstCache &ic, int64_t gsite, int64_t total_sites,
+                                       int want_state, int64_t &h)
+{
+    if (gsite >= total_sites) return -1;
+    const int64_t w = gsite >> 3;
+    int i;
+    if (e.ninst <= kInstCache) {
+        i = find_instance(ic.d, ic.n, w, [](const InstDesc &d) { return d.warp_begin; });
+        if (ic.state[i] != want_state) return -1;
+    } else {
+        i = find_instance(e.inst, e.ninst, w, [](const InstDesc &d) { return d.warp_begin; });
+        if (e.state[i] != want_state) return -1;
+    }
+    h = gsite - inst_at(e, ic, i).warp_begin * 8;
+    return i;
+}
+
 // Persistent variant with register prefetch: every warp walks a strided list of 8-site tiles and
 // issues the loads of tile t+1 (its lane's two links, and the W column in refine mode) into
 // registers before it computes tile t, so each warp keeps a tile's worth of loads in flight
@@ -102,13 +147,19 @@ struct TileRegs {
 };
 
 template <typename R, bool SITE_W>
-__device__ __forceinline__ void fetch_tile_regs(const EngineDev &e, int64_t tile, int parity, int want_state,
-                                                TileRegs<R> &t)
+__device__ __forceinline__ void fetch_tile_regs(const EngineDev &e, const InstCache &ic, int64_t tile, int parity,
+                                                int want_state, TileRegs<R> &t)
 {
     t.inst = -1;
-    const int i = find_instance(e.inst, e.ninst, tile, [](const InstDesc &d) { return d.warp_begin; });
-    if (e.state[i] != want_state) return;
-    const InstDesc &d = e.inst[i];
+    int i;
+    if (e.ninst <= kInstCache) {
+        i = find_instance(ic.d, ic.n, tile, [](const InstDesc &d) { return d.warp_begin; });
+        if (ic.state[i] != want_state) return;
+    } else {
+        i = find_instance(e.inst, e.ninst, tile, [](const InstDesc &d) { return d.warp_begin; });
+        if (e.state[i] != want_state) return;
+    }
+    const InstDesc &d = inst_at(e, ic, i);
     const int lane = threadIdx.x & 31, mu = lane >> 3;
     t.inst = i;
     t.h = (tile - d.warp_begin) * 8 + (lane & 7);
@@ -131,18 +182,20 @@ __global__ void __launch_bounds__(128) k_batched_pass_rp(EngineDev e, int64_t to
                                                          int want_state)
 {
     static_assert(GAUGE != COULOMB, "Coulomb slices use k_batched_pass");
+    __shared__ InstCache ic;
+    fill_inst_cache(e, ic);
     const int mu = (threadIdx.x & 31) >> 3;
     const int64_t stride = (int64_t)gridDim.x * 4;
     int64_t tile = (int64_t)blockIdx.x * 4 + (threadIdx.x >> 5);
     TileRegs<R> cur;
     cur.inst = -1;
-    if (tile < total_warps) fetch_tile_regs<R, SITE_W>(e, tile, parity, want_state, cur);
+    if (tile < total_warps) fetch_tile_regs<R, SITE_W>(e, ic, tile, parity, want_state, cur);
     for (; tile < total_warps; tile += stride) {
         TileRegs<R> nxt;
         nxt.inst = -1;
-        if (tile + stride < total_warps) fetch_tile_regs<R, SITE_W>(e, tile + stride, parity, want_state, nxt);
+        if (tile + stride < total_warps) fetch_tile_regs<R, SITE_W>(e, ic, tile + stride, parity, want_state, nxt);
         if (cur.inst >= 0) {
-            const InstDesc &d = e.inst[cur.inst];
+            const InstDesc &d = inst_at(e, ic, cur.inst);
             Link<R> up, dn;
             unpack12(up, cur.up);
             reconstruct(up);
@@ -587,21 +640,11 @@ __device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 
-// the instance and half-lattice site of global site index gsite, or -1 (inactive / past the end)
-__device__ __forceinline__ int site_of(const EngineDev &e, int64_t gsite, int64_t total_sites, int want_state,
-                                       int64_t &h)
-{
-    if (gsite >= total_sites) return -1;
-    const int i = find_instance(e.inst, e.ninst, gsite >> 3, [](const InstDesc &d) { return d.warp_begin; });
-    if (e.state[i] != want_state) return -1;
-    h = gsite - e.inst[i].warp_begin * 8;
-    return i;
-}
-
 template <bool SITE_W>
-__device__ __forceinline__ void prefetch_site(const EngineDev &e, int i, int64_t h, int parity, uint4 *stage)
+__device__ __forceinline__ void prefetch_site(const EngineDev &e, const InstCache &ic, int i, int64_t h, int parity,
+                                              uint4 *stage)
 {
-    const InstDesc &d = e.inst[i];
+    const InstDesc &d = inst_at(e, ic, i);
     int32_t c[4];
     site_coords(d.g, h, parity, c);
     const int64_t s = h + (parity ? d.g.Vh : 0);
@@ -643,25 +686,27 @@ __global__ void __launch_bounds__(128, 2) k_batched_pass_site_staged(EngineDev e
 {
     static_assert(GAUGE != COULOMB, "Coulomb slices use k_batched_pass");
     extern __shared__ uint4 smem[];
+    __shared__ InstCache ic;
+    fill_inst_cache(e, ic);
     constexpr int SL = SiteStage<SITE_W>::slots;
     uint4 *stages[2] = {smem, smem + SL * 128};
     const int64_t total_sites = total_warps * 8;
     const int64_t stride = (int64_t)gridDim.x * 128;
     int64_t gsite = (int64_t)blockIdx.x * 128 + threadIdx.x;
     int64_t h = 0;
-    int inst = site_of(e, gsite, total_sites, want_state, h);
-    if (inst >= 0) prefetch_site<SITE_W>(e, inst, h, parity, stages[0]);
+    int inst = site_of(e, ic, gsite, total_sites, want_state, h);
+    if (inst >= 0) prefetch_site<SITE_W>(e, ic, inst, h, parity, stages[0]);
     cp_async_commit();
     int cur = 0;
     // every thread of the block runs the same number of iterations (the tile loop is uniform)
     for (int64_t tile0 = (int64_t)blockIdx.x * 128; tile0 < total_sites; tile0 += stride) {
         int64_t hn = 0;
-        const int next = site_of(e, gsite + stride, total_sites, want_state, hn);
-        if (next >= 0) prefetch_site<SITE_W>(e, next, hn, parity, stages[cur ^ 1]);
+        const int next = site_of(e, ic, gsite + stride, total_sites, want_state, hn);
+        if (next >= 0) prefetch_site<SITE_W>(e, ic, next, hn, parity, stages[cur ^ 1]);
         cp_async_commit();
         cp_async_wait<1>();
         if (inst >= 0) {
-            const InstDesc &d = e.inst[inst];
+            const InstDesc &d = inst_at(e, ic, inst);
             int32_t c[4];
             site_coords(d.g, h, parity, c);
             const int64_t s = h + (parity ? d.g.Vh : 0);

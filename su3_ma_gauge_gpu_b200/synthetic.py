@@ -185,3 +185,22 @@ def smooth_config(size, eps: float, seed: int, transform: bool = True, dtype=np.
 def hot_config(size, seed: int, dtype=np.float64):
     """Haar-random links (the 8^4 plain-method configuration)."""
     return to_gpupattern(hot_links(size, np.random.default_rng(seed)), size, dtype)
+
+
+def gpupattern_to_timeslices(U: np.ndarray, size) -> np.ndarray:
+    """GpuPattern array -> GpuPatternTimeslice array (access_pattern/GpuPatternTimeslice.hxx:57-62):
+    slice t at offset 72*Vs*t is the GpuPattern array of its {1, Nx, Ny, Nz} lattice, whose
+    parity split is by x+y+z.  This is the layout a Coulomb context imports."""
+    nt, nx, ny, nz = (int(v) for v in size)
+    vs = nx * ny * nz
+    v = nt * vs
+    t, x, y, z = (a.reshape(-1) for a in np.meshgrid(np.arange(nt), np.arange(nx), np.arange(ny), np.arange(nz),
+                                                     indexing="ij"))
+    l = ((t * nx + x) * ny + y) * nz + z
+    s_full = l // 2 + ((t + x + y + z) % 2) * (v // 2)
+    ls = (x * ny + y) * nz + z
+    s_slice = ls // 2 + ((x + y + z) % 2) * (vs // 2)
+    src = np.asarray(U).reshape(72, v)
+    out = np.empty((nt, 72, vs), dtype=src.dtype)
+    out[t, :, s_slice] = src[:, s_full].T
+    return out.reshape(-1)

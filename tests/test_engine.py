@@ -224,8 +224,11 @@ def test_thread_per_site_pass_matches_direct(cuda, gauge, algo):
                 gf.store(i, o)
                 res.append(o)
             outs.append(res)
+    # U1xU1 microcanonical steps divide by the norm of a two-component quaternion, which is small
+    # at some sites of a Haar-transformed field: there one rounding difference grows to ~2e-5
+    tol = 1e-4 if (gauge, algo) == ("u1xu1", "micro") else 1e-5
     for a, b in zip(*outs):
-        assert np.abs(a - b).max() < 1e-5
+        assert np.abs(a - b).max() < tol
 
 
 def test_autotune_picks_a_shape(cuda):

@@ -31,6 +31,14 @@ def _file_bytes(U, size, fmt, file_dtype=np.float64):
     return body
 
 
+def test_timeslice_converter_matches_oracle():
+    from su3_ma_gauge_gpu_b200 import synthetic as S
+
+    for size in SIZES:
+        U = F.random_links(size, 3)
+        assert np.array_equal(S.gpupattern_to_timeslices(U, size), F.gpu_to_timeslice(U, size))
+
+
 def test_python_api_argument_checks(tmp_path):
     with pytest.raises(ValueError):
         files.read_config(tmp_path / "x", "NOPE", (2, 2, 2, 2), np.zeros(72 * 16))
