@@ -107,10 +107,10 @@ int gf_stats_destroy(gf_stats *st);
  * device-wide synchronisation is not acceptable.  Its reduction scratch is a fixed array in
  * device memory (about 1 MiB, held by every GPU that loads the library until the process
  * exits), so lattices are limited to 16,777,216 sites (64^4); larger ones return
- * GF_ERR_INVALID.  The first call on a device looks up that array's device address (do it
- * once before latency matters).  All calls share the one array: calls whose kernels overlap on
- * the GPU (different streams or threads at the same time) race and must be serialised by the
- * caller.  Blocking, like gf_stats_generate; stopping = GF_MAX or GF_AVERAGE. */
+ * GF_ERR_INVALID.  The first call on a device looks up that array's device address: make it
+ * once before latency matters, and before any stream capture.  All calls share the one array:
+ * calls whose kernels overlap on the GPU (different streams or threads at the same time) race
+ * and must be serialised by the caller.  Blocking, like gf_stats_generate; stopping = GF_MAX or GF_AVERAGE. */
 int gf_quality_noalloc(int gauge, int real, const void *U, const int32_t size[4], int stopping,
                        void *stream, double *gff, double *theta);
 

@@ -209,6 +209,11 @@ __device__ __forceinline__ void upd_or(R a[4], float omega)
 {
     const R ai_sq = a[1] * a[1] + a[2] * a[2] + a[3] * a[3];
     const R a0_sq = a[0] * a[0];
+    if (!(a0_sq + ai_sq > (R)0)) {  // no coupling (every contribution cancelled): leave the site
+        a[0] = 1;
+        a[1] = a[2] = a[3] = 0;
+        return;
+    }
     const R b = (omega * a0_sq + ai_sq) / (a0_sq + ai_sq);
     const R c = rsq(a0_sq + b * b * ai_sq);
     const R bc = b * c;
@@ -225,6 +230,11 @@ __device__ __forceinline__ void upd_micro(R a[4])
     const R ai_sq = a[1] * a[1] + a[2] * a[2] + a[3] * a[3];
     const R a0_sq = a[0] * a[0];
     const R n = a0_sq + ai_sq;
+    if (!(n > (R)0)) {  // no coupling: the reflection is undefined, leave the site
+        a[0] = 1;
+        a[1] = a[2] = a[3] = 0;
+        return;
+    }
     const R b = (R)2. * a[0] / n;
     a[0] = (a0_sq - ai_sq) / n;
     a[1] *= b;
@@ -234,29 +244,50 @@ __device__ __forceinline__ void upd_micro(R a[4])
 
 // Kennedy-Pendleton heat-bath, SaUpdate::calculateUpdate (SaUpdate.hxx:103-146).  The literal
 // types follow the reference (double constants, cospi of a double argument), so the FP32
-// variant promotes where the reference promotes.  Every rejection loop is bounded; the bound
-// (2^16 draws) is never reached for finite input since each draw is accepted with probability
-// >= 1e-4 in the inner loops and > 1/2 in the outer one.
+// variant promotes where the reference promotes.  Every rejection loop is bounded (2^16 draws).
+// The inner loops accept with probability >= 0.9999 per draw; the outer one accepts rarely when
+// p0 = T/|a| is large (a site whose subgroup coupling |a| is tiny against the temperature), and
+// there the reference would keep drawing.  Such a site -- the outer bound exhausted, or |a| = 0
+// -- takes a0 from the p0 -> infinity limit of the same distribution, the Haar measure (density
+// proportional to sqrt(1 - a0^2), sampled by rejection), instead of the unaccepted 1 - delta,
+// whose square root below would be NaN for delta > 2.
 template <typename R>
 __device__ __forceinline__ void upd_sa(R a[4], float temperature, Rng<R> &rng)
 {
     R e0 = a[0], e1 = -a[1], e2 = -a[2], e3 = -a[3];
-    const R dk = rsq(e0 * e0 + e1 * e1 + e2 * e2 + e3 * e3);
+    const R nrm2 = e0 * e0 + e1 * e1 + e2 * e2 + e3 * e3;
+    const bool flat = !(nrm2 > (R)0);  // no coupling: the local distribution is Haar
+    const R dk = flat ? (R)1 : rsq(nrm2);
+    if (flat) {
+        e0 = 1;
+        e1 = e2 = e3 = 0;
+    }
     const R p0 = dk * temperature;
-    R r1, r2, r3, r4, delta;
+    R r1, r2, r3, r4, delta = 0;
+    bool accepted = false;
     int guard = 0;
-    do {
-        int g1 = 0, g2 = 0;
-        do { r1 = rng.rand(); } while (r1 < 0.0001 && ++g1 < 65536);
-        r1 = -lg(r1) * p0;
-        do { r2 = rng.rand(); } while (r2 < 0.0001 && ++g2 < 65536);
-        r2 = -lg(r2) * p0;
-        r3 = (R)cospi(2.0 * (double)rng.rand());
-        r3 = r3 * r3;
-        delta = r2 + r1 * r3;
-        r4 = rng.rand();
-    } while (r4 * r4 > (1.0 - 0.5 * delta) && ++guard < 65536);
-    const R a0 = (R)(1.0 - delta);
+    if (!flat) {
+        do {
+            int g1 = 0, g2 = 0;
+            do { r1 = rng.rand(); } while (r1 < 0.0001 && ++g1 < 65536);
+            r1 = -lg(r1) * p0;
+            do { r2 = rng.rand(); } while (r2 < 0.0001 && ++g2 < 65536);
+            r2 = -lg(r2) * p0;
+            r3 = (R)cospi(2.0 * (double)rng.rand());
+            r3 = r3 * r3;
+            delta = r2 + r1 * r3;
+            r4 = rng.rand();
+            accepted = !(r4 * r4 > (1.0 - 0.5 * delta));
+        } while (!accepted && ++guard < 65536);
+    }
+    R a0 = (R)(1.0 - delta);
+    if (!accepted) {
+        int g = 0;
+        do {
+            a0 = (R)(2.0 * rng.rand() - 1.0);
+            r4 = rng.rand();
+        } while (r4 * r4 > (R)1 - a0 * a0 && ++g < 64);
+    }
     const R cos_theta = (R)(2.0 * rng.rand() - 1.0);
     const R sin_theta = (R)sqrt(1.0 - (double)(cos_theta * cos_theta));
     const R sin_alpha = sq((R)(1 - a0 * a0));

@@ -583,15 +583,15 @@ __global__ void __launch_bounds__(WARPS * 32) k_batched_pass_staged(EngineDev e,
     extern __shared__ uint4 smem[];
     constexpr int NCH = Chunks<R>::per_lane;
     const int w = threadIdx.x >> 5;
-    uint4 *stages[2] = {smem + (2 * w) * NCH * 32, smem + (2 * w + 1) * NCH * 32};
+    uint4 *const wbase = smem + (2 * w) * NCH * 32;  // this warp's two stages, NCH * 32 chunks apart
     const int64_t stride = (int64_t)gridDim.x * WARPS;
     int64_t tile = (int64_t)blockIdx.x * WARPS + w;
     int cur = 0;
-    TileRef t = tile < total_warps ? prefetch_tile<R>(e, tile, parity, want_state, stages[0]) : TileRef{-1, 0, 0, 0};
+    TileRef t = tile < total_warps ? prefetch_tile<R>(e, tile, parity, want_state, wbase) : TileRef{-1, 0, 0, 0};
     cp_async_commit();
     for (; tile < total_warps; tile += stride) {
         const int64_t nt = tile + stride;
-        const TileRef n = nt < total_warps ? prefetch_tile<R>(e, nt, parity, want_state, stages[cur ^ 1])
+        const TileRef n = nt < total_warps ? prefetch_tile<R>(e, nt, parity, want_state, wbase + (cur ^ 1) * NCH * 32)
                                            : TileRef{-1, 0, 0, 0};
         cp_async_commit();
         cp_async_wait<1>();
@@ -599,8 +599,8 @@ __global__ void __launch_bounds__(WARPS * 32) k_batched_pass_staged(EngineDev e,
             const InstDesc &d = e.inst[t.inst];
             const int mu = (threadIdx.x & 31) >> 3;
             Link<R> up, dn;
-            unstage_link<R>(stages[cur], 0, up);
-            unstage_link<R>(stages[cur], Chunks<R>::per_link, dn);
+            unstage_link<R>(wbase + cur * NCH * 32, 0, up);
+            unstage_link<R>(wbase + cur * NCH * 32, Chunks<R>::per_link, dn);
             Rng<R> rng;
             if (ALGO == ALG_SA || ALGO == ALG_SR || ALGO == ALG_RANDOM)
                 rng.init(ref_rng_tid(t.h), p.seed + (uint32_t)t.inst, p.counter);
@@ -609,7 +609,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_batched_pass_staged(EngineDev e,
             store_link<R>(f, t.s, mu, up);
             store_link<R>(f, t.sd, mu, dn);
         }
-        __syncwarp();  // every lane is done with stages[cur] before it is refilled
+        __syncwarp();  // every lane is done with the current stage before it is refilled
         t = n;
         cur ^= 1;
     }
@@ -689,20 +689,23 @@ __global__ void __launch_bounds__(128, 2) k_batched_pass_site_staged(EngineDev e
     __shared__ InstCache ic;
     fill_inst_cache(e, ic);
     constexpr int SL = SiteStage<SITE_W>::slots;
-    uint4 *stages[2] = {smem, smem + SL * 128};
+    // stage k starts at smem + k * SL * 128 (pointer arithmetic: an array of the two stage
+    // pointers indexed by the loop's stage bit would live in local memory)
     const int64_t total_sites = total_warps * 8;
     const int64_t stride = (int64_t)gridDim.x * 128;
     int64_t gsite = (int64_t)blockIdx.x * 128 + threadIdx.x;
     int64_t h = 0;
     int inst = site_of(e, ic, gsite, total_sites, want_state, h);
-    if (inst >= 0) prefetch_site<SITE_W>(e, ic, inst, h, parity, stages[0]);
+    if (inst >= 0) prefetch_site<SITE_W>(e, ic, inst, h, parity, smem);
     cp_async_commit();
     int cur = 0;
     // every thread of the block runs the same number of iterations (the tile loop is uniform)
     for (int64_t tile0 = (int64_t)blockIdx.x * 128; tile0 < total_sites; tile0 += stride) {
         int64_t hn = 0;
         const int next = site_of(e, ic, gsite + stride, total_sites, want_state, hn);
-        if (next >= 0) prefetch_site<SITE_W>(e, ic, next, hn, parity, stages[cur ^ 1]);
+        uint4 *const stage_cur = smem + cur * (SL * 128);
+        uint4 *const stage_next = smem + (cur ^ 1) * (SL * 128);
+        if (next >= 0) prefetch_site<SITE_W>(e, ic, next, hn, parity, stage_next);
         cp_async_commit();
         cp_async_wait<1>();
         if (inst >= 0) {
@@ -713,14 +716,14 @@ __global__ void __launch_bounds__(128, 2) k_batched_pass_site_staged(EngineDev e
             Link<float> up[4], dn[4];
 #pragma unroll
             for (int mu = 0; mu < 4; mu++) {
-                unstage_link_f32(stages[cur], mu * 3, up[mu]);
-                unstage_link_f32(stages[cur], 12 + mu * 3, dn[mu]);
+                unstage_link_f32(stage_cur, mu * 3, up[mu]);
+                unstage_link_f32(stage_cur, 12 + mu * 3, dn[mu]);
                 reconstruct(up[mu]);
                 reconstruct(dn[mu]);
             }
             Cx<float> wc[2][3];
             if (SITE_W) {
-                const float2 *ws = reinterpret_cast<const float2 *>(stages[cur] + 24 * 128);
+                const float2 *ws = reinterpret_cast<const float2 *>(stage_cur + 24 * 128);
 #pragma unroll
                 for (int q = 0; q < 6; q++) {
                     const float2 v = ws[((q >> 1) * 128 + threadIdx.x) * 2 + (q & 1)];
