@@ -1,0 +1,267 @@
+"""One lattice over several GPUs: t-slabs with a halo exchange per parity pass.
+
+The reference's multi-GPU driver splits ONE lattice into slabs of timeslices, one per MPI rank,
+and around every parity pass of the boundary sites sends the temporal links of the boundary
+slice forward and returns them updated (apps/MultiGPU_MPI/MultiGPU_MPI_Communicator.hxx:351-430).
+This module does the same with torch.distributed point-to-point messages (NCCL over NVLink on
+GPUs, gloo on CPU) around the library's own parity pass, unchanged:
+
+* rank r owns the timeslices [r*T, (r+1)*T) (T = Nt / world, even) and keeps them as slices
+  2 .. T+1 of a local lattice of extent T + 2, whose slices 0 and 1 are a halo.  Site parity is
+  the same locally and globally because every slab starts at an even t.
+* A site of the first owned slice reads its down temporal link U_t(x - t) from halo slice 1; no
+  other owned site reads the halo.  In the pass of parity p those links belong to the
+  parity-(1-p) sites of slice 1 -- the last owned slice of rank r-1, where the pass of parity p
+  does not touch them.  So before the pass rank r-1 sends them (rows 0 and 1: Vs/2 x 12 reals,
+  the reference's message) and after it rank r returns them, updated, into rank r-1's last slice.
+* The pass also updates the halo sites of parity p; they read wrapped or stale neighbours and
+  write only halo links and the wrapped parity-(1-p) temporal links of the last owned slice --
+  exactly the links the returned message overwrites.  Nothing owned is left corrupted.
+
+The message is tiny next to the pass (Vs/2 x 12 reals per boundary, about 2.6 MB for 48^3 in
+FP32), so it is sent with plain send/recv; the functional and theta are summed with all_reduce.
+Only deterministic updates (overrelaxation, microcanonical) give the single-lattice result bit
+for bit: the heat-bath draws its Philox numbers by local site index.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def _site_index(size, t, x, y, z):
+    """Parity-split index of sites (arrays of coordinates) in a lattice of extents `size`."""
+    nt, nx, ny, nz = size
+    v = nt * nx * ny * nz
+    l = ((t * nx + x) * ny + y) * nz + z
+    return l // 2 + ((t + x + y + z) % 2) * (v // 2)
+
+
+class TSlab:
+    """The slab of rank `rank` out of `world` for a lattice of extents `size` = (Nt, Nx, Ny, Nz).
+
+    Arrays are GpuPattern arrays (18 reals per link) of the local lattice `self.local_size`:
+    CUDA tensors with the library's plugin pass, or any array type the injected pass accepts."""
+
+    def __init__(self, size, rank: int, world: int):
+        nt, nx, ny, nz = (int(v) for v in size)
+        if world < 1 or not 0 <= rank < world or nt % world or (nt // world) % 2:
+            raise ValueError("Nt must split into `world` slabs of an even number of timeslices")
+        self.size = (nt, nx, ny, nz)
+        self.rank, self.world = rank, world
+        self.T = nt // world
+        self.t0 = rank * self.T
+        self.local_size = (self.T + 2, nx, ny, nz)
+        self.V = (self.T + 2) * nx * ny * nz
+        self.Vs = nx * ny * nz
+        x, y, z = (a.reshape(-1) for a in np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij"))
+        self._xyz = (x, y, z)
+        V = self.V
+        ls = self.local_size
+        # reals 0..11 (rows 0, 1) of U_t at local slice `t` for the sites of parity `q`, in (x, y, z) order
+        def t_rows(t, q):
+            sel = ((t + x + y + z) % 2) == q
+            s = _site_index(ls, np.full(sel.sum(), t), x[sel], y[sel], z[sel])
+            return (s[:, None] + V * np.arange(12)[None, :]).reshape(-1)  # mu = 0: offset 18*0*V
+        # before / after the pass of parity p the parity-(1-p) links move between slabs
+        self._halo = {p: t_rows(1, 1 - p) for p in (0, 1)}
+        self._last = {p: t_rows(self.T + 1, 1 - p) for p in (0, 1)}
+        # owned sites (slices 2 .. T+1) in local parity-split order, and their global indices
+        tl = np.repeat(np.arange(2, self.T + 2), self.Vs)
+        xx, yy, zz = (np.tile(a, self.T) for a in (x, y, z))
+        self._owned_local = _site_index(ls, tl, xx, yy, zz)
+        self._owned_global = _site_index(self.size, tl - 2 + self.t0, xx, yy, zz)
+        self._owned_mask = np.zeros(V, dtype=bool)
+        self._owned_mask[self._owned_local] = True
+
+    # ---- moving whole fields between the global array and the slabs (set-up, checks) ----------
+    def scatter(self, Uglob, xp=np):
+        """Local array of this rank from the global GpuPattern array: owned slices, halo slices
+        filled from the two slices before t0 (so the halo holds unitary links)."""
+        nt = self.size[0]
+        Vg = int(np.prod(self.size))
+        x, y, z = self._xyz
+        Ug = Uglob.reshape(72, Vg)
+        out = xp.zeros((72, self.V), dtype=Uglob.dtype) if xp is np else None
+        loc_list, glob_list = [], []
+        for tl in range(self.T + 2):
+            tg = (self.t0 + tl - 2) % nt
+            loc_list.append(_site_index(self.local_size, np.full(self.Vs, tl), x, y, z))
+            glob_list.append(_site_index(self.size, np.full(self.Vs, tg), x, y, z))
+        loc = np.concatenate(loc_list)
+        glob = np.concatenate(glob_list)
+        if xp is np:
+            out[:, loc] = Ug[:, glob]
+            return out.reshape(-1)
+        import torch
+
+        out = torch.zeros((72, self.V), dtype=Uglob.dtype, device=Uglob.device)
+        out[:, torch.as_tensor(loc, device=Uglob.device)] = Ug[:, torch.as_tensor(glob, device=Uglob.device)]
+        return out.reshape(-1)
+
+    def gather_into(self, Ulocal, Uglob):
+        """Write this rank's owned slices into the global GpuPattern array (in place)."""
+        Vg = int(np.prod(self.size))
+        Ug = Uglob.reshape(72, Vg)
+        Ul = Ulocal.reshape(72, self.V)
+        if isinstance(Uglob, np.ndarray):
+            Ug[:, self._owned_global] = Ul[:, self._owned_local]
+        else:
+            import torch
+
+            dev = Uglob.device
+            Ug[:, torch.as_tensor(self._owned_global, device=dev)] = Ul[:, torch.as_tensor(self._owned_local,
+                                                                                         device=dev)]
+
+    # ---- the exchange ---------------------------------------------------------------------------
+    def _idx(self, which, p, U):
+        idx = which[p]
+        if isinstance(U, np.ndarray):
+            return idx
+        import torch
+
+        key = (id(which), p, str(U.device))
+        cache = self.__dict__.setdefault("_tidx", {})
+        if key not in cache:
+            cache[key] = torch.as_tensor(idx, device=U.device)
+        return cache[key]
+
+    def boundary_out(self, U, p):
+        """Before the pass of parity p: what goes to rank r+1 (its halo)."""
+        return U[self._idx(self._last, p, U)]
+
+    def halo_in(self, U, p, msg):
+        U[self._idx(self._halo, p, U)] = msg
+
+    def halo_out(self, U, p):
+        """After the pass of parity p: the updated halo links that go back to rank r-1."""
+        return U[self._idx(self._halo, p, U)]
+
+    def boundary_in(self, U, p, msg):
+        U[self._idx(self._last, p, U)] = msg
+
+    def owned_sum(self, per_site):
+        """Sum of a per-site array (local parity-split order) over the owned sites."""
+        if isinstance(per_site, np.ndarray):
+            return float(per_site[self._owned_mask].sum())
+        import torch
+
+        mask = self.__dict__.get("_tmask")
+        if mask is None or mask.device != per_site.device:
+            mask = torch.as_tensor(self._owned_mask, device=per_site.device)
+            self._tmask = mask
+        return float(per_site[mask].sum().item())
+
+
+def parity_pass(slab: TSlab, U, parity: int, run_pass, group=None):
+    """One parity pass of the whole lattice, this rank's share: halo in, run_pass(U, local_size,
+    parity) on the local lattice, updated halo back.  Ring point-to-point messages through
+    torch.distributed; with one rank the ring is a local copy."""
+    p = parity
+    if slab.world == 1:
+        slab.halo_in(U, p, slab.boundary_out(U, p))
+        run_pass(U, slab.local_size, p)
+        slab.boundary_in(U, p, slab.halo_out(U, p))
+        return
+    import torch
+    import torch.distributed as dist
+
+    nxt, prv = (slab.rank + 1) % slab.world, (slab.rank - 1) % slab.world
+    host = isinstance(U, np.ndarray)  # host arrays (CPU runs): messages travel as CPU tensors
+
+    def ring(msg, to, frm):
+        send = torch.from_numpy(np.ascontiguousarray(msg)) if host else msg.contiguous()
+        recv = torch.empty_like(send)
+        reqs = dist.batch_isend_irecv([dist.P2POp(dist.isend, send, to, group),
+                                       dist.P2POp(dist.irecv, recv, frm, group)])
+        for r in reqs:
+            r.wait()
+        return recv.numpy() if host else recv
+
+    slab.halo_in(U, p, ring(slab.boundary_out(U, p), nxt, prv))
+    run_pass(U, slab.local_size, p)
+    slab.boundary_in(U, p, ring(slab.halo_out(U, p), prv, nxt))
+
+
+def refresh_halo(slab: TSlab, U, group=None):
+    """Bring the halo's temporal links of BOTH parities up to date (the sweep keeps only those the
+    next pass reads current) -- needed before the functional and theta, whose first owned slice
+    reads every down temporal link."""
+    if slab.world == 1:
+        for p in (0, 1):
+            slab.halo_in(U, p, slab.boundary_out(U, p))
+        return
+    import torch
+    import torch.distributed as dist
+
+    host = isinstance(U, np.ndarray)
+    nxt, prv = (slab.rank + 1) % slab.world, (slab.rank - 1) % slab.world
+    for p in (0, 1):
+        msg = slab.boundary_out(U, p)
+        send = torch.from_numpy(np.ascontiguousarray(msg)) if host else msg.contiguous()
+        recv = torch.empty_like(send)
+        reqs = dist.batch_isend_irecv([dist.P2POp(dist.isend, send, nxt, group),
+                                       dist.P2POp(dist.irecv, recv, prv, group)])
+        for r in reqs:
+            r.wait()
+        slab.halo_in(U, p, recv.numpy() if host else recv)
+
+
+def quality(slab: TSlab, U, per_site, group=None):
+    """(sum of the functional terms, sum of the theta terms) over the whole lattice: per_site(U,
+    local_size) returns the per-site arrays of the local lattice; owned sites are summed and the
+    sums all-reduced.  Normalise like the single-lattice quality."""
+    refresh_halo(slab, U, group)
+    g, a = per_site(U, slab.local_size)
+    sums = [slab.owned_sum(g), slab.owned_sum(a)]
+    if slab.world > 1:
+        import torch
+        import torch.distributed as dist
+
+        t = torch.tensor(sums, dtype=torch.float64)
+        if not isinstance(U, np.ndarray):
+            t = t.to(U.device)
+        dist.all_reduce(t, group=group)
+        sums = [float(v) for v in t.cpu()]
+    return sums[0], sums[1]
+
+
+def emulate_refresh_halo(slabs, Us):
+    world = len(slabs)
+    for p in (0, 1):
+        outs = [slabs[r].boundary_out(Us[r], p) for r in range(world)]
+        for r in range(world):
+            slabs[r].halo_in(Us[r], p, outs[(r - 1) % world])
+
+
+def emulate_parity_pass(slabs, Us, parity: int, run_pass):
+    """The same pass for all ranks of one process (one GPU, or CPU), ranks one after the other:
+    every message is a copy.  No rank waits on another inside a kernel."""
+    world = len(slabs)
+    outs = [slabs[r].boundary_out(Us[r], parity) for r in range(world)]  # fancy indexing copies
+    for r in range(world):
+        slabs[r].halo_in(Us[r], parity, outs[(r - 1) % world])
+    for r in range(world):
+        run_pass(Us[r], slabs[r].local_size, parity)
+    backs = [slabs[r].halo_out(Us[r], parity) for r in range(world)]
+    for r in range(world):
+        slabs[r].boundary_in(Us[r], parity, backs[(r + 1) % world])
+
+
+def gpu_or_pass(omega: float = 1.7, gauge: str = "landau", precision: str = "double"):
+    """run_pass for parity_pass: the library's in-place plugin pass (gf_or_step) on the local
+    lattice, CUDA tensors.  Coulomb's per-timeslice pass is not a slab pass and is refused."""
+    from . import plugins
+
+    cls = {"landau": plugins.LandauKernelsSU3, "mag": plugins.MAGKernelsSU3,
+           "u1xu1": plugins.U1xU1KernelsSU3}.get(gauge)
+    if cls is None:
+        raise ValueError("t-slabs are for the 4D gauges (landau, mag, u1xu1)")
+    kernels = {}
+
+    def run(U, local_size, parity):
+        k = kernels.get(local_size)
+        if k is None:
+            k = kernels[local_size] = cls(local_size, precision)
+        k.orStep(0, 0, U, None, parity, omega)
+
+    return run

@@ -1,0 +1,143 @@
+"""One lattice split into t-slabs (su3_ma_gauge_gpu_b200.tslab): the halo exchange around every
+parity pass reproduces the single-lattice sweep bit for bit (overrelaxation is deterministic and
+each site update reads only its 8 links).  CPU: the oracle plays the pass, ranks emulated in one
+process and as world-size-2 gloo process groups; GPU: the library's plugin pass, ranks emulated
+one after the other on one device."""
+import os
+import socket
+
+import numpy as np
+import pytest
+
+import _oracle as O
+from su3_ma_gauge_gpu_b200 import synthetic as S
+from su3_ma_gauge_gpu_b200.tslab import (TSlab, emulate_parity_pass, emulate_refresh_halo, gpu_or_pass, parity_pass,
+                                        quality)
+
+SIZE = (8, 4, 6, 4)
+
+
+def _oracle_pass(U, size, parity):
+    O.step(U, size, O.LANDAU, O.OR, parity, 1.7, nthreads=2)
+
+
+def _reference(U, nsweeps):
+    R = U.copy()
+    for _ in range(nsweeps):
+        for p in (0, 1):
+            _oracle_pass(R, SIZE, p)
+    return R
+
+
+def test_slab_geometry_checks():
+    with pytest.raises(ValueError):
+        TSlab((8, 4, 4, 4), 0, 3)  # 8 does not split in 3
+    with pytest.raises(ValueError):
+        TSlab((6, 4, 4, 4), 0, 2)  # slabs of 3 timeslices: odd
+    s = TSlab(SIZE, 1, 2)
+    assert s.local_size == (6, 4, 6, 4) and s.t0 == 4
+    assert s.boundary_out(np.arange(72 * s.V, dtype=float), 0).size == s.Vs // 2 * 12
+
+
+@pytest.mark.parametrize("world", [1, 2, 4])
+def test_emulated_slabs_match_single_lattice(world):
+    U, _ = S.smooth_config(SIZE, 0.3, 31)
+    slabs = [TSlab(SIZE, r, world) for r in range(world)]
+    Us = [s.scatter(U) for s in slabs]
+    for _ in range(3):
+        for p in (0, 1):
+            emulate_parity_pass(slabs, Us, p, _oracle_pass)
+    out = np.zeros_like(U)
+    for s, L in zip(slabs, Us):
+        s.gather_into(L, out)
+    R = _reference(U, 3)
+    assert np.array_equal(out, R)
+    # the functional and theta summed over the owned sites of the slabs, halos refreshed first
+    emulate_refresh_halo(slabs, Us)
+    _, _, g, a = O.quality(R, SIZE, O.LANDAU, per_site=True)
+    gs = sum(s.owned_sum(O.quality(L, s.local_size, O.LANDAU, per_site=True)[2]) for s, L in zip(slabs, Us))
+    ts = sum(s.owned_sum(O.quality(L, s.local_size, O.LANDAU, per_site=True)[3]) for s, L in zip(slabs, Us))
+    assert gs == pytest.approx(float(g.sum()), rel=1e-13)
+    assert ts == pytest.approx(float(a.sum()), rel=1e-11)
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _rank(rank, world, port, U, q):
+    import datetime
+
+    import torch.distributed as dist
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        slab = TSlab(SIZE, rank, world)
+        L = slab.scatter(U)
+        for _ in range(2):
+            for p in (0, 1):
+                parity_pass(slab, L, p, _oracle_pass)
+        sums = quality(slab, L, lambda A, size: O.quality(A, size, O.LANDAU, per_site=True)[2:])
+        out = np.zeros_like(U)
+        slab.gather_into(L, out)
+        q.put((rank, out, sums))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gloo_two_ranks_match_single_lattice():
+    import torch.multiprocessing as mp
+
+    U, _ = S.smooth_config(SIZE, 0.3, 32)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank, args=(r, 2, port, U, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = [q.get(timeout=180) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    res = {r: (o, s) for r, o, s in got}
+    out = np.zeros_like(U)
+    for r in range(2):
+        sl = TSlab(SIZE, r, 2)
+        out.reshape(72, -1)[:, sl._owned_global] = res[r][0].reshape(72, -1)[:, sl._owned_global]
+    R = _reference(U, 2)
+    assert np.array_equal(out, R)
+    _, _, g, a = O.quality(R, SIZE, O.LANDAU, per_site=True)
+    for r in range(2):  # every rank holds the all-reduced sums
+        assert res[r][1][0] == pytest.approx(float(g.sum()), rel=1e-13)
+        assert res[r][1][1] == pytest.approx(float(a.sum()), rel=1e-11)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("world", [1, 2])
+def test_gpu_slabs_match_plugin_pass(cuda, world):
+    """The library's own pass on every slab, ranks one after the other on one GPU, against the
+    same pass on the whole lattice."""
+    torch = cuda
+    from su3_ma_gauge_gpu_b200 import LandauKernelsSU3
+
+    U, _ = S.smooth_config(SIZE, 0.3, 33)
+    dU = torch.from_numpy(U).cuda()
+    k = LandauKernelsSU3(SIZE, "double")
+    for _ in range(3):
+        for p in (0, 1):
+            k.orStep(0, 0, dU, None, p, 1.7)
+    slabs = [TSlab(SIZE, r, world) for r in range(world)]
+    Us = [s.scatter(torch.from_numpy(U).cuda(), xp=torch) for s in slabs]
+    run = gpu_or_pass(1.7)
+    for _ in range(3):
+        for p in (0, 1):
+            emulate_parity_pass(slabs, Us, p, run)
+    out = torch.zeros_like(dU)
+    for s, L in zip(slabs, Us):
+        s.gather_into(L, out)
+    assert torch.equal(out, dU)
