@@ -391,7 +391,11 @@ def run_coulomb48(args):
 def run_mag48(args):
     """Maximal Abelian gauge on a 48^4 lattice, U = exp(i*0.5*H) under a Haar gauge transform: 3000
     SA sweeps (Philox heat-bath, geometric T 1.4 -> 0.01), then OR omega = 1.7, FP32 working copy
-    with the gauge transformation tracked (refine mode), FP64 polish to theta < 1e-12."""
+    with the gauge transformation tracked (refine mode), FP64 polish to theta < 1e-12.  Then the
+    U(1)xU(1) check: 500 OR sweeps of the U1xU1 app's residual diagonal gauge fixing on the
+    MAG-fixed field, whose MAG functional sum |U_jj|^2 such diagonal transformations must leave
+    unchanged while the U1xU1 functional rises (the U1xU1 theta is the full-matrix Landau measure,
+    which diagonal transformations cannot drive to zero)."""
     import numpy as np
     import torch
 
@@ -407,12 +411,27 @@ def run_mag48(args):
                      precision=1e-12, switch_theta=1e-9, check_precision=args.check, reproject=100, seed=9)
     with GaugeFixer([size], gauge="mag", mixed="refine", stream=stream) as gf:
         ms, reps = _timed_fix(gf, [dU], sched, args.steps, args.warmup, stream)
+        gf.store(0, dU)  # the MAG-fixed field, reunitarised, in place of the input
     r = reps[0]
     V = int(np.prod(size))
+    u1 = Schedule(or_max_iter=500, precision=1e-12, switch_theta=1e-9, check_precision=args.check, reproject=100,
+                  micro_updates=0)
+    with GaugeFixer([size], gauge="u1xu1", mixed="refine", stream=stream) as gu:
+        gu.load(0, dU)
+        f_u1_before = float(gu.quality()[0][0])
+        ms_u1, reps_u1 = _timed_fix(gu, [dU], u1, 1, 0, stream)
+        gu.store(0, dU)
+    with GaugeFixer([size], gauge="mag", mixed=False, stream=stream) as gq:
+        gq.load(0, dU)
+        f_after = float(gq.quality()[0][0])
+    ru = reps_u1[0]
     print(json.dumps({"workload": "mag48", "ms_per_fix": ms, "sa_sweeps": r.sa_sweeps, "or_sweeps": r.or_sweeps,
                       "or_sweeps_fp64": r.or_sweeps_fp64, "theta": r.theta, "F": r.gff, "converged": r.converged,
                       "footprint_fp32_12_gb": V * 4 * 48 / 1e9,
-                      "gsite_updates_per_s": V * (r.or_sweeps + r.sa_sweeps) / (ms * 1e-3) / 1e9}))
+                      "gsite_updates_per_s": V * (r.or_sweeps + r.sa_sweeps) / (ms * 1e-3) / 1e9,
+                      "u1xu1_check": {"ms": ms_u1, "or_sweeps": ru.or_sweeps, "F_u1_before": f_u1_before,
+                                      "F_u1_after": ru.gff, "F_mag_after": f_after,
+                                      "F_mag_rel_change": abs(f_after - r.gff) / abs(r.gff)}}))
 
 
 def main():

@@ -360,6 +360,35 @@ def test_mag_app_schedule(cuda):
     assert rep.gff > g0[0]  # the MAG functional increased
 
 
+def test_u1xu1_fix_after_mag_keeps_the_mag_functional(cuda):
+    """The residual U(1)xU(1) gauge fixing after MAG applies only diagonal transformations, which
+    leave the MAG functional sum |U_jj|^2 unchanged while they raise the U1xU1 functional: fix MAG,
+    then 200 U1xU1 OR sweeps, and compare.  (The U1xU1 theta is the full-matrix Landau measure,
+    U1xU1KernelsSU3.hxx:114-191, which diagonal transformations cannot drive to zero.)"""
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer, Schedule
+
+    size = (4, 4, 4, 8)
+    U, _ = S.smooth_config(size, 0.3, 91)
+    sch = Schedule(or_max_iter=3000, precision=1e-12, switch_theta=1e-9, check_precision=20, reproject=20,
+                   micro_updates=0)
+    out = np.zeros_like(U)
+    with GaugeFixer([size], gauge="mag", mixed=False) as gf:
+        gf.load(0, U)
+        rep = gf.fix(sch)[0]
+        gf.store(0, out)
+    assert rep.converged
+    with GaugeFixer([size], gauge="u1xu1", mixed=False) as gu:
+        gu.load(0, out)
+        f0, _ = gu.quality()
+        ru = gu.fix(Schedule(or_max_iter=200, precision=1e-12, check_precision=20, reproject=20, micro_updates=0))[0]
+        gu.store(0, out)
+    assert ru.or_sweeps == 200 and ru.gff > f0[0]
+    with GaugeFixer([size], gauge="mag", mixed=False) as gq:
+        gq.load(0, out)
+        g, _ = gq.quality()
+    assert g[0] == pytest.approx(rep.gff, rel=1e-12)
+
+
 def test_stall_rule_off_keeps_mag_in_fp32(cuda):
     """With stall_checks = 0 the switch waits for theta < switch_theta, which FP32 MAG never
     reaches: the run stays in FP32 and ends at the sweep cap (the old behaviour)."""
