@@ -29,6 +29,28 @@ def _reference(U, nsweeps):
     return R
 
 
+@pytest.mark.parametrize("gauge,algo", [(O.MAG, O.OR), (O.U1XU1, O.OR), (O.LANDAU, O.MICRO), (O.MAG, O.MICRO)])
+def test_emulated_slabs_other_gauges_and_updates(gauge, algo):
+    """Every deterministic update of the 4D gauges reads only a site's 8 links: the slabs give
+    the single-lattice result bit for bit for MAG and U1xU1, OR and microcanonical."""
+    U, _ = S.smooth_config(SIZE, 0.3, 35)
+
+    def run(A, size, parity):
+        O.step(A, size, gauge, algo, parity, 1.7, nthreads=2)
+
+    slabs = [TSlab(SIZE, r, 2) for r in range(2)]
+    Us = [s.scatter(U) for s in slabs]
+    R = U.copy()
+    for _ in range(2):
+        for p in (0, 1):
+            emulate_parity_pass(slabs, Us, p, run)
+            run(R, SIZE, p)
+    out = np.zeros_like(U)
+    for s, L in zip(slabs, Us):
+        s.gather_into(L, out)
+    assert np.array_equal(out, R)
+
+
 def test_slab_geometry_checks():
     with pytest.raises(ValueError):
         TSlab((8, 4, 4, 4), 0, 3)  # 8 does not split in 3
