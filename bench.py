@@ -123,29 +123,63 @@ class ClockSampler:
 
 def cpu_oracle():
     sys.path.insert(0, str(ROOT / "tests"))
-    import _oracle  # the oracle is loaded only for the CPU-baseline leg and the reference arm
+    import _oracle  # the oracle is loaded only for the baseline leg and the reference arm
 
     return _oracle
 
 
-def cpu_or_rate(U, size, budget_s: float):
-    """FP64 OR sweeps of the C restatement on all host cores for about budget_s seconds."""
+def host_cpu_info() -> dict:
+    """The host threads this process may use, the CPU model and the load average around a CPU timing
+    (the host cores of a GPU box are shared with other users' jobs)."""
+    try:
+        threads = len(os.sched_getaffinity(0))
+    except Exception:
+        threads = os.cpu_count() or 1
+    model = "unknown"
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+    except Exception:
+        pass
+    return {"threads": threads, "nproc": os.cpu_count(), "model": model, "loadavg_1m": os.getloadavg()[0]}
+
+
+CPU_SWEEPS = 20
+CPU_WARMUP = 3
+
+
+def cpu_or_sweeps(U, size, sweeps: int = CPU_SWEEPS, warmup: int = CPU_WARMUP) -> dict:
+    """FP64 OR sweeps (omega = 1.7, both parities) of the C restatement of the reference's device code
+    on every host thread this process may use: `warmup` untimed sweeps, then `sweeps` sweeps timed one
+    by one.  The bench's cpu_baseline and the reference arm both time through this function."""
     O = cpu_oracle()
-    n_thr = os.cpu_count() or 1
-    V = O.volume(size)
+    info = host_cpu_info()
+    n_thr = info["threads"]
     W = U.copy()
-    t0 = time.perf_counter()
-    for parity in (0, 1):
-        O.step(W, size, O.LANDAU, O.OR, parity, 1.7, nthreads=n_thr)
-    one = time.perf_counter() - t0
-    n = max(1, int(budget_s / max(one, 1e-6)) - 1)
-    t0 = time.perf_counter()
-    for _ in range(n):
+
+    def sweep():
         for parity in (0, 1):
             O.step(W, size, O.LANDAU, O.OR, parity, 1.7, nthreads=n_thr)
-    t = time.perf_counter() - t0
-    return {"value": V * n / t / 1e9, "unit": UNIT, "cores": n_thr, "kind": "port",
-            "sample": f"{n} FP64 OR sweeps (omega=1.7) of the 32^4 input on {n_thr} host threads"}
+
+    for _ in range(warmup):
+        sweep()
+    times = []
+    for _ in range(sweeps):
+        t0 = time.perf_counter()
+        sweep()
+        times.append(time.perf_counter() - t0)
+    info["loadavg_1m_after"] = os.getloadavg()[0]
+    V = O.volume(size)
+    mean = sum(times) / len(times)
+    return {"value": V / mean / 1e9, "unit": UNIT, "cores": n_thr, "kind": "port",
+            "sweeps": len(times), "warmup": warmup, "s_per_sweep": {"mean": mean, "median": statistics.median(times),
+                                                                   "min": min(times), "max": max(times)},
+            "host": info,
+            "sample": f"{len(times)} FP64 OR sweeps (omega=1.7, after {warmup} untimed) of the 32^4 input, C restatement "
+                      f"of the reference's device code (the reference has no CPU path), OpenMP over the sites of a "
+                      f"parity on {n_thr} host threads ({info['model']})"}
 
 
 def run_reference(args):
@@ -154,36 +188,76 @@ def run_reference(args):
         return
     from su3_ma_gauge_gpu_b200 import synthetic as S
 
-    O = cpu_oracle()
-    U, _ = S.smooth_config(SIZE, EPS, 1234)
-    V = O.volume(SIZE)
-    n_thr = os.cpu_count() or 1
-    W = U.copy()
+    dev = None
+    try:
+        import torch
 
-    def step():
-        for parity in (0, 1):
-            O.step(W, SIZE, O.LANDAU, O.OR, parity, 1.7, nthreads=n_thr)
-
-    for _ in range(args.warmup):
-        step()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        step()
-    t = (time.perf_counter() - t0) / args.steps
-    val = V / t / 1e9
+        dev = "cuda" if torch.cuda.is_available() else None
+    except Exception:
+        pass
+    U, _ = S.smooth_config(SIZE, EPS, 1234, device=dev)
+    r = cpu_or_sweeps(U, SIZE, sweeps=args.steps, warmup=args.warmup)
+    val = r["value"]
     line = {
         "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "warmup": args.warmup, "ms_per_step": r["s_per_sweep"]["mean"] * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "Landau OR sweep of a 32^4 SU(3) lattice (eps=0.3 smooth field under a Haar "
                                "gauge transform), FP64; one step = one sweep (both parities)",
                    "lattice": list(SIZE)},
-        "cpu_baseline": {"value": val, "unit": UNIT, "cores": n_thr, "kind": "port",
-                         "sample": "C restatement of the reference device code (the reference has no CPU path), "
-                                   f"OpenMP over sites, {n_thr} threads, one FP64 OR sweep per step"},
+        "cpu_baseline": r,
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def reference_gpu_leg(dU_in, gpu_id, fixes) -> dict | None:
+    """The reference's own CUDA kernels on the same GPU (oracle/_ref, built from the reference tree for
+    the 32^4 extent with its Makefile's flags), as the checker of the headline: the Landau app's
+    overrelaxation loop (apps/LandauGaugeFixingSU3_4D.cu:244-271) in FP64 on the same input to
+    theta < 1e-12, and the per-sweep time of its FP32 and FP64 OR kernels under a clock record.
+    `fixes` maps a name to this library's gf_report of the same input; their functional errors
+    against the reference path are returned.  None when the reference kernels were not built."""
+    import numpy as np
+    import torch
+
+    O = cpu_oracle()
+    lib64 = O.refgpu("libref_gpu_X32T32_f64.so")
+    lib32 = O.refgpu("libref_gpu_X32T32_f32.so")
+    if lib64 is None or lib32 is None:
+        return None
+    V = O.volume(SIZE)
+    nn = torch.from_numpy(O.refgpu_neighbours(lib64, SIZE)).cuda()
+    out = {}
+    clocks = ClockSampler(gpu_id)
+    dU = dU_in.clone()
+    F, th, n, ms = O.refgpu_or_loop(lib64, 0, dU.data_ptr(), nn.data_ptr(), 1.7, float(np.float32(1e-12)), 20, 100)
+    out["fix_fp64"] = {"F": F, "theta": th, "or_sweeps": n, "ms": ms,
+                       "note": "reference kernels driven by the Landau app's OR loop; its quality check is the "
+                               "reference's single-thread reduction, inside the time"}
+    for prec, lib, dt in (("fp32", lib32, torch.float32), ("fp64", lib64, torch.float64)):
+        x = dU_in.to(dt)
+        for _ in range(3):
+            for p in (0, 1):
+                lib.refgpu_step(0, 0, x.data_ptr(), None, nn.data_ptr(), p, 1.7, 0, 0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(20):
+            for p in (0, 1):
+                lib.refgpu_step(0, 0, x.data_ptr(), None, nn.data_ptr(), p, 1.7, 0, 0)
+        e1.record()
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 20
+        nb = 4 if prec == "fp32" else 8
+        out[f"or_sweep_{prec}"] = {"ms_per_sweep": t, "gsite_updates_per_s": V / (t * 1e-3) / 1e9,
+                                   "GBs_192B_per_site": 192 * nb * V / (t * 1e-3) / 1e9}
+        del x
+    out["clocks"] = clocks.stop()
+    out["F_rel_err_vs_reference"] = {k: abs(r.gff - F) / abs(F) for k, r in fixes.items()}
+    del dU, nn
+    torch.cuda.empty_cache()
+    return out
 
 
 def run_profile_target(nsweeps: int, mode: str = "fast"):
@@ -249,94 +323,15 @@ def run_launch_list(args):
 GRIBOV_LATTICES = [((12, 12, 12, 12), 24), ((16, 16, 16, 16), 24), ((40, 20, 20, 20), 16)]
 
 
-def run_gribov(args):
-    """64 random-gauge-start Gribov copies of three uneven lattices (24 x 12^4, 24 x 16^4,
-    16 x 20^3x40, eps = 0.3 smooth fields), all fixed in ONE batch: every parity pass is one
-    launch over all copies, per-copy convergence decided on the device, check chunks replayed
-    from CUDA graphs, autotuned pass shape.  Reports copies/s and the best functional per lattice."""
-    import numpy as np
-    import torch
-
-    from su3_ma_gauge_gpu_b200 import synthetic as S
-    from su3_ma_gauge_gpu_b200.engine import GaugeFixer, Schedule
-
-    bases = [S.smooth_config(size, EPS, 500 + k, device="cuda")[0] for k, (size, _) in enumerate(GRIBOV_LATTICES)]
-    dbases = [torch.from_numpy(b).cuda() for b in bases]
-    sizes, owner = [], []
-    for k, (size, n) in enumerate(GRIBOV_LATTICES):
-        sizes += [size] * n
-        owner += [k] * n
-    stream = torch.cuda.Stream()
-    gf = GaugeFixer(sizes, mixed=True, stream=stream)
-    sched = Schedule(random_trafo=1, seed=77, or_max_iter=20000, precision=1e-12, switch_theta=1e-9,
-                     check_precision=args.check, reproject=100, micro_updates=0)
-
-    def step():
-        for i, k in enumerate(owner):
-            gf.load(i, dbases[k])
-        return gf.fix(sched)
-
-    reps = None
-    for _ in range(args.warmup):
-        reps = step()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        reps = step()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / args.steps
-    vols = [int(np.prod(s)) for s in sizes]
-    updates = sum(v * r.or_sweeps for v, r in zip(vols, reps))
-    best = {}
-    for (size, _), k in zip(GRIBOV_LATTICES, range(len(GRIBOV_LATTICES))):
-        fs = [r.gff for r, o in zip(reps, owner) if o == k]
-        best["x".join(map(str, size))] = {"best_F": max(fs), "min_F": min(fs), "copies": len(fs)}
-    gf.close()
-    print(json.dumps({
-        "workload": "gribov", "copies": len(sizes), "total_sites": sum(vols), "ms_per_batch": ms,
-        "copies_per_s": len(sizes) / (ms * 1e-3), "gsite_updates_per_s": updates / (ms * 1e-3) / 1e9,
-        "all_converged": all(r.converged for r in reps), "max_theta": max(r.theta for r in reps),
-        "or_sweeps": {"min": min(r.or_sweeps for r in reps), "max": max(r.or_sweeps for r in reps)},
-        "best_per_lattice": best}))
-
-
-def run_plain8(args):
-    """The 8^4 plain-method configuration: Haar-random links, FP64 (the reference's full 18-real
-    array in, out), OR omega = 1.7 to theta < 1e-12, at most 20000 sweeps; timed per fix."""
-    import numpy as np
-    import torch
-
-    from su3_ma_gauge_gpu_b200 import synthetic as S
-    from su3_ma_gauge_gpu_b200.engine import GaugeFixer, Schedule
-
-    size = (8, 8, 8, 8)
-    U = torch.from_numpy(S.hot_config(size, 4242)).cuda()
-    out = torch.empty_like(U)
-    stream = torch.cuda.Stream()
-    gf = GaugeFixer([size], mixed=False, stream=stream)
-    sched = Schedule(or_max_iter=20000, precision=1e-12, check_precision=args.check, reproject=100,
-                     micro_updates=0)
-    rep = None
-    for _ in range(args.warmup):
-        gf.load(0, U)
-        rep = gf.fix(sched)[0]
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        gf.load(0, U)
-        rep = gf.fix(sched)[0]
-        gf.store(0, out)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / args.steps
-    V = int(np.prod(size))
-    gf.close()
-    print(json.dumps({"workload": "plain8", "ms_per_fix": ms, "or_sweeps": rep.or_sweeps, "theta": rep.theta,
-                      "F": rep.gff, "converged": rep.converged, "us_per_sweep": ms * 1e3 / max(1, rep.or_sweeps),
-                      "gsite_updates_per_s": V * rep.or_sweeps / (ms * 1e-3) / 1e9}))
+def _clocked(fn, gpu_id=None):
+    """Run fn() -> dict under an nvidia-smi clock record; the record goes into the dict."""
+    clocks = ClockSampler(gpu_id)
+    try:
+        r = fn()
+    finally:
+        clk = clocks.stop()
+    r["clocks"] = clk
+    return r
 
 
 def _timed_fix(gf, loads, sched, steps, warmup, stream):
@@ -360,78 +355,190 @@ def _timed_fix(gf, loads, sched, steps, warmup, stream):
     return e0.elapsed_time(e1) / max(1, steps), reps
 
 
-def run_coulomb48(args):
-    """Coulomb gauge on a 48^3 x 16 lattice (eps = 0.3 smooth field under a Haar gauge transform):
-    all 16 timeslices fixed as independent instances in the same launches; per slice 500 SA
-    sweeps, T 1.0 -> 0.01, a microcanonical sweep after every 3rd SA sweep, then OR omega = 1.7
-    to theta < 1e-12; FP32 bulk, FP64 polish, FP64 reductions."""
+def run_gribov(args, steps=None, warmup=None):
+    """64 random-gauge-start Gribov copies of three uneven lattices (24 x 12^4, 24 x 16^4,
+    16 x 20^3x40, eps = 0.3 smooth fields), all fixed in ONE batch: every parity pass is one
+    launch over all copies, per-copy convergence decided on the device, check chunks replayed
+    from CUDA graphs, autotuned pass shape, refine mixed precision (FP32 working copies on an
+    FP64 master).  Reports copies/s and the best functional per lattice."""
     import numpy as np
     import torch
 
     from su3_ma_gauge_gpu_b200 import synthetic as S
     from su3_ma_gauge_gpu_b200.engine import GaugeFixer, Schedule
 
+    steps = args.steps if steps is None else steps
+    warmup = args.warmup if warmup is None else warmup
+    dbases = [S.smooth_config(size, EPS, 500 + k, device="cuda", as_tensor=True)[0]
+              for k, (size, _) in enumerate(GRIBOV_LATTICES)]
+    sizes, owner = [], []
+    for k, (size, n) in enumerate(GRIBOV_LATTICES):
+        sizes += [size] * n
+        owner += [k] * n
+    stream = torch.cuda.Stream()
+    sched = Schedule(random_trafo=1, seed=77, or_max_iter=20000, precision=1e-12, switch_theta=1e-9,
+                     check_precision=args.check, reproject=100, micro_updates=0)
+    with GaugeFixer(sizes, mixed="refine", stream=stream) as gf:
+        gf.load(0, dbases[0])
+        gf.autotune()
+        ms, reps = _timed_fix(gf, [dbases[k] for k in owner], sched, steps, warmup, stream)
+    vols = [int(np.prod(s)) for s in sizes]
+    updates = sum(v * r.or_sweeps for v, r in zip(vols, reps))
+    best = {}
+    for k, (size, _) in enumerate(GRIBOV_LATTICES):
+        fs = sorted((r.gff for r, o in zip(reps, owner) if o == k), reverse=True)
+        best["x".join(map(str, size))] = {"best_F": fs[0], "second_F": fs[1], "min_F": fs[-1], "copies": len(fs),
+                                          "best_minus_second_rel": (fs[0] - fs[1]) / fs[0]}
+    return {"workload": "gribov", "mixed": "refine", "copies": len(sizes), "total_sites": sum(vols),
+            "steps": steps, "warmup": warmup, "ms_per_batch": ms, "copies_per_s": len(sizes) / (ms * 1e-3),
+            "gsite_updates_per_s": updates / (ms * 1e-3) / 1e9, "all_converged": all(r.converged for r in reps),
+            "max_theta": max(r.theta for r in reps),
+            "or_sweeps": {"min": min(r.or_sweeps for r in reps), "max": max(r.or_sweeps for r in reps)},
+            "best_per_lattice": best}
+
+
+def run_plain8(args, steps=None, warmup=None):
+    """The 8^4 plain-method configuration: Haar-random links, FP64 (the reference's full 18-real
+    array in, out), OR omega = 1.7 to theta < 1e-12, at most 20000 sweeps; timed per fix."""
+    import numpy as np
+    import torch
+
+    from su3_ma_gauge_gpu_b200 import synthetic as S
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer, Schedule
+
+    steps = args.steps if steps is None else steps
+    warmup = args.warmup if warmup is None else warmup
+    size = (8, 8, 8, 8)
+    U = torch.from_numpy(S.hot_config(size, 4242)).cuda()
+    out = torch.empty_like(U)
+    stream = torch.cuda.Stream()
+    sched = Schedule(or_max_iter=20000, precision=1e-12, check_precision=args.check, reproject=100,
+                     micro_updates=0)
+    with GaugeFixer([size], mixed=False, stream=stream) as gf:
+        gf.load(0, U)
+        gf.autotune()
+        rep = None
+        for _ in range(warmup):
+            gf.load(0, U)
+            rep = gf.fix(sched)[0]
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(max(1, steps)):
+            gf.load(0, U)
+            rep = gf.fix(sched)[0]
+            gf.store(0, out)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / max(1, steps)
+    V = int(np.prod(size))
+    return {"workload": "plain8", "steps": steps, "warmup": warmup, "ms_per_fix": ms, "or_sweeps": rep.or_sweeps,
+            "theta": rep.theta, "F": rep.gff, "converged": rep.converged,
+            "us_per_sweep": ms * 1e3 / max(1, rep.or_sweeps),
+            "gsite_updates_per_s": V * rep.or_sweeps / (ms * 1e-3) / 1e9}
+
+
+def run_coulomb48(args, steps=None, warmup=None):
+    """Coulomb gauge on a 48^3 x 16 lattice (eps = 0.3 smooth field under a Haar gauge transform):
+    all 16 timeslices fixed as independent instances in the same launches; per slice 500 SA
+    sweeps, T 1.0 -> 0.01, a microcanonical sweep after every 3rd SA sweep, then OR omega = 1.7
+    to theta < 1e-12; refine mixed precision (FP32 working copy, FP64 master), FP64 reductions."""
+    import numpy as np
+    import torch
+
+    from su3_ma_gauge_gpu_b200 import synthetic as S
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer, Schedule
+
+    steps = args.steps if steps is None else steps
+    warmup = args.warmup if warmup is None else warmup
     size = (16, 48, 48, 48)
     U, _ = S.smooth_config(size, EPS, 4848, device="cuda")
     T = torch.from_numpy(S.gpupattern_to_timeslices(U, size)).cuda()
+    del U
     stream = torch.cuda.Stream()
     sched = Schedule(sa_steps=500, sa_min=0.01, sa_max=1.0, micro_updates=1, micro_every=3, or_max_iter=20000,
                      precision=1e-12, switch_theta=1e-9, check_precision=args.check, reproject=100, seed=7)
-    with GaugeFixer([size], gauge="coulomb", mixed=True, stream=stream) as gf:
-        ms, reps = _timed_fix(gf, [T], sched, args.steps, args.warmup, stream)
+    with GaugeFixer([size], gauge="coulomb", mixed="refine", stream=stream) as gf:
+        gf.load(0, T)
+        gf.autotune()
+        ms, reps = _timed_fix(gf, [T], sched, steps, warmup, stream)
     V = int(np.prod(size))
     sweeps = sum(r.or_sweeps + r.sa_sweeps for r in reps) / len(reps)
-    print(json.dumps({"workload": "coulomb48x16", "ms_per_fix": ms, "timeslices": len(reps),
-                      "all_converged": all(r.converged for r in reps), "max_theta": max(r.theta for r in reps),
-                      "or_sweeps": {"min": min(r.or_sweeps for r in reps), "max": max(r.or_sweeps for r in reps)},
-                      "sa_sweeps": reps[0].sa_sweeps, "mean_F": float(np.mean([r.gff for r in reps])),
-                      "gsite_updates_per_s": V * sweeps / (ms * 1e-3) / 1e9}))
+    return {"workload": "coulomb48x16", "mixed": "refine", "steps": steps, "warmup": warmup, "ms_per_fix": ms,
+            "timeslices": len(reps), "all_converged": all(r.converged for r in reps),
+            "max_theta": max(r.theta for r in reps),
+            "or_sweeps": {"min": min(r.or_sweeps for r in reps), "max": max(r.or_sweeps for r in reps)},
+            "sa_sweeps": reps[0].sa_sweeps, "mean_F": float(np.mean([r.gff for r in reps])),
+            "gsite_updates_per_s": V * sweeps / (ms * 1e-3) / 1e9}
 
 
-def run_mag48(args):
+def run_mag48(args, steps=None, warmup=None):
     """Maximal Abelian gauge on a 48^4 lattice, U = exp(i*0.5*H) under a Haar gauge transform: 3000
     SA sweeps (Philox heat-bath, geometric T 1.4 -> 0.01), then OR omega = 1.7, FP32 working copy
     with the gauge transformation tracked (refine mode), FP64 polish to theta < 1e-12.  Then the
     U(1)xU(1) check: 500 OR sweeps of the U1xU1 app's residual diagonal gauge fixing on the
     MAG-fixed field, whose MAG functional sum |U_jj|^2 such diagonal transformations must leave
     unchanged while the U1xU1 functional rises (the U1xU1 theta is the full-matrix Landau measure,
-    which diagonal transformations cannot drive to zero)."""
+    which diagonal transformations cannot drive to zero).  The input is generated on the GPU and
+    stays there."""
     import numpy as np
     import torch
 
     from su3_ma_gauge_gpu_b200 import synthetic as S
     from su3_ma_gauge_gpu_b200.engine import GaugeFixer, Schedule
 
+    steps = args.steps if steps is None else steps
+    warmup = args.warmup if warmup is None else warmup
+    stages = {}
+    t0 = time.perf_counter()
     size = (48, 48, 48, 48)
-    U, _ = S.smooth_config(size, 0.5, 4849, device="cuda")
-    dU = torch.from_numpy(U).cuda()
-    del U
+    dU, _ = S.smooth_config(size, 0.5, 4849, device="cuda", as_tensor=True)
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    stages["input_s"] = time.perf_counter() - t0
     stream = torch.cuda.Stream()
     sched = Schedule(sa_steps=3000, sa_min=0.01, sa_max=1.4, sa_geometric=1, micro_updates=0, or_max_iter=20000,
                      precision=1e-12, switch_theta=1e-9, check_precision=args.check, reproject=100, seed=9)
+    t0 = time.perf_counter()
     with GaugeFixer([size], gauge="mag", mixed="refine", stream=stream) as gf:
-        ms, reps = _timed_fix(gf, [dU], sched, args.steps, args.warmup, stream)
+        gf.load(0, dU)
+        gf.autotune()
+        ms, reps = _timed_fix(gf, [dU], sched, steps, warmup, stream)
         gf.store(0, dU)  # the MAG-fixed field, reunitarised, in place of the input
+    stages["mag_fix_s"] = time.perf_counter() - t0
     r = reps[0]
     V = int(np.prod(size))
     u1 = Schedule(or_max_iter=500, precision=1e-12, switch_theta=1e-9, check_precision=args.check, reproject=100,
                   micro_updates=0)
+    t0 = time.perf_counter()
     with GaugeFixer([size], gauge="u1xu1", mixed="refine", stream=stream) as gu:
         gu.load(0, dU)
         f_u1_before = float(gu.quality()[0][0])
+        gu.autotune()
         ms_u1, reps_u1 = _timed_fix(gu, [dU], u1, 1, 0, stream)
         gu.store(0, dU)
+    stages["u1xu1_s"] = time.perf_counter() - t0
     with GaugeFixer([size], gauge="mag", mixed=False, stream=stream) as gq:
         gq.load(0, dU)
         f_after = float(gq.quality()[0][0])
     ru = reps_u1[0]
-    print(json.dumps({"workload": "mag48", "ms_per_fix": ms, "sa_sweeps": r.sa_sweeps, "or_sweeps": r.or_sweeps,
-                      "or_sweeps_fp64": r.or_sweeps_fp64, "theta": r.theta, "F": r.gff, "converged": r.converged,
-                      "footprint_fp32_12_gb": V * 4 * 48 / 1e9,
-                      "gsite_updates_per_s": V * (r.or_sweeps + r.sa_sweeps) / (ms * 1e-3) / 1e9,
-                      "u1xu1_check": {"ms": ms_u1, "or_sweeps": ru.or_sweeps, "F_u1_before": f_u1_before,
-                                      "F_u1_after": ru.gff, "F_mag_after": f_after,
-                                      "F_mag_rel_change": abs(f_after - r.gff) / abs(r.gff)}}))
+    return {"workload": "mag48", "mixed": "refine", "steps": steps, "warmup": warmup, "ms_per_fix": ms,
+            "sa_sweeps": r.sa_sweeps, "or_sweeps": r.or_sweeps, "or_sweeps_fp64": r.or_sweeps_fp64, "theta": r.theta,
+            "F": r.gff, "converged": r.converged, "footprint_fp32_12_gb": V * 4 * 48 / 1e9,
+            "gsite_updates_per_s": V * (r.or_sweeps + r.sa_sweeps) / (ms * 1e-3) / 1e9,
+            "u1xu1_check": {"ms": ms_u1, "or_sweeps": ru.or_sweeps, "F_u1_before": f_u1_before,
+                            "F_u1_after": ru.gff, "F_mag_after": f_after,
+                            "F_mag_rel_change": abs(f_after - r.gff) / abs(r.gff)},
+            "wall_s": stages}
+
+
+EXTRA_CONFIGS = {
+    # name: (runner, timed steps, warm-up fixes) for the default run's per-configuration keys
+    "plain8": (run_plain8, 3, 1),
+    "coulomb48x16": (run_coulomb48, 1, 1),
+    "gribov64": (run_gribov, 1, 1),
+    "mag48": (run_mag48, 1, 0),
+}
 
 
 def main():
@@ -455,6 +562,9 @@ def main():
                     help="landau32: the headline 32^4 mixed-precision fix; gribov: 64 random-gauge copies of "
                          "uneven lattices in one batch; plain8: the 8^4 Haar-random FP64 plain fix; coulomb48: "
                          "48^3x16 Coulomb, 16 timeslices batched, 500 SA + OR; mag48: 48^4 MAG, 3000 SA + OR")
+    ap.add_argument("--extras", default="all",
+                    help="comma-separated configurations to run after the headline on a single GPU and report as "
+                         "extra keys (plain8, coulomb48x16, gribov64, mag48), 'all' or 'none'")
     ap.add_argument("--profile-mode", default="fast", choices=["fast", "refine"])
     ap.add_argument("--launch-list", action="store_true",
                     help="one headline step without graphs, warm-up or clock sampling, for ncu's launch list")
@@ -471,17 +581,9 @@ def main():
     if args.launch_list:
         run_launch_list(args)
         return
-    if args.workload == "gribov":
-        run_gribov(args)
-        return
-    if args.workload == "plain8":
-        run_plain8(args)
-        return
-    if args.workload == "coulomb48":
-        run_coulomb48(args)
-        return
-    if args.workload == "mag48":
-        run_mag48(args)
+    runners = {"gribov": run_gribov, "plain8": run_plain8, "coulomb48": run_coulomb48, "mag48": run_mag48}
+    if args.workload in runners:
+        print(json.dumps(_clocked(lambda: runners[args.workload](args))), flush=True)
         return
 
     import numpy as np
@@ -653,9 +755,28 @@ def main():
                 "algorithmic_bytes_per_launch": Vh * kern[dom]["bytes_per_site_update"], "peak_kind": peak_kind,
                 "per_precision": kern}
 
+    # the checker and the baselines, on rank 0 of a single-GPU run only: the reference's own kernels on
+    # this GPU, and the C restatement of its device code on the host cores
+    ref_gpu = None
     cpu = None
+    extras = {}
     if rank == 0 and world == 1:
-        cpu = cpu_or_rate(U_host, SIZE, args.cpu_budget)
+        fixes = {"mixed": rep}
+        if res64 is not None:
+            fixes["fp64"] = res64
+        ref_gpu = reference_gpu_leg(dU_in, gpu_id, fixes)
+        cpu = cpu_or_sweeps(U_host, SIZE)
+        names = list(EXTRA_CONFIGS) if args.extras == "all" else \
+            [n for n in args.extras.split(",") if n in EXTRA_CONFIGS]
+        del dU_in, dU_out
+        torch.cuda.empty_cache()
+        for name in names:
+            fn, st, wu = EXTRA_CONFIGS[name]
+            try:
+                extras[name] = _clocked(lambda: fn(args, steps=st, warmup=wu), gpu_id)
+            except Exception as e:  # a failing extra configuration is reported, not fatal for the headline
+                extras[name] = {"error": f"{type(e).__name__}: {e}"}
+            torch.cuda.empty_cache()
 
     if rank != 0:
         if dist is not None:
@@ -694,7 +815,11 @@ def main():
             "F_rel_err_vs_fp64": (abs(rep.gff - res64.gff) / abs(res64.gff)) if res64 else None,
             "F_pre_transform": f0,
             "F_rel_vs_pre_transform": (rep.gff - f0) / f0,
+            "reference_kernels": ref_gpu,
+            "F_rel_err_vs_reference": (ref_gpu or {}).get("F_rel_err_vs_reference"),
+            "fp64_gsite_updates_per_s": (V * res64.or_sweeps / (ms64 * 1e-3) / 1e9) if res64 else None,
         },
+        "configs": extras,
     }
     print(json.dumps(line), flush=True)
     if dist is not None:

@@ -53,6 +53,10 @@ extern "C" {
 const char *gf_last_error_string(void);
 /* Library version string. */
 const char *gf_version(void);
+/* Compute capability the device code that runs on the current device was built for, as
+ * major * 10 + minor (100 for sm_100a), from cudaFuncGetAttributes.  No counterpart in the
+ * reference (its apps are built per architecture by their Makefile); needs a GPU. */
+int gf_binary_arch(int *arch);
 
 /* ---- plugin level: one parity pass, in place on a GpuPattern device array ------------------
  * stream: a cudaStream_t, or NULL for the default stream.  Launches are asynchronous.
@@ -107,8 +111,10 @@ int gf_stats_destroy(gf_stats *st);
  * device-wide synchronisation is not acceptable.  Its reduction scratch is a fixed array in
  * device memory (about 1 MiB, held by every GPU that loads the library until the process
  * exits), so lattices are limited to 16,777,216 sites (64^4); larger ones return
- * GF_ERR_INVALID.  The first call on a device looks up that array's device address: make it
- * once before latency matters, and before any stream capture.  All calls share the one array:
+ * GF_ERR_INVALID.  Every call looks up that array's device address on the caller's current
+ * device (nothing is kept across calls, so a device reset in between is harmless); the first
+ * call on a device may load the library's module there: make it once before latency matters,
+ * and before any stream capture.  All calls share the one array:
  * calls whose kernels overlap on the GPU (different streams or threads at the same time) race
  * and must be serialised by the caller.  Blocking, like gf_stats_generate; stopping = GF_MAX or GF_AVERAGE. */
 int gf_quality_noalloc(int gauge, int real, const void *U, const int32_t size[4], int stopping,
@@ -140,8 +146,10 @@ typedef struct gf_ctx_params {
                               polish; 2 ("refine"): an FP64 master field plus an FP32 working copy
                               that also accumulates the gauge transformation W(x); at the switch
                               the master becomes W(x) U(x) W(x+mu)^dagger, so rounding in the FP32
-                              phase never moves the field off its gauge orbit (not for GF_COULOMB:
-                              GF_ERR_UNSUPPORTED) */
+                              phase never moves the field off its gauge orbit.  A GF_COULOMB slice
+                              keeps its W in its own temporal planes: the fold applies the working
+                              copy's W32 to the master's spatial links and multiplies it into the
+                              master's W64, which gf_export applies to the temporal links */
     void *stream;          /* cudaStream_t to run on, or NULL for a stream of the context's own */
 } gf_ctx_params;
 

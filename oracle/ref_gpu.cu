@@ -162,3 +162,58 @@ int refgpu_project(int timeslice, Real *U)
 }
 
 }  // extern "C"
+
+#ifndef REFGPU_U1
+namespace {
+
+// The overrelaxation phase of the apps' per-copy loop, on the reference's own kernels:
+// apps/LandauGaugeFixingSU3_4D.cu:244-271 (MAG: apps/MAGaugeFixingSU3_4D.cu:300-329) -- orStep for
+// parity 0 and 1; projectSU3 when i % reproject == 0; generateGaugeQuality when
+// i % checkprecision == 0, leaving the loop once A < precision (a float, as the apps' option);
+// the closing projectSU3.  One GaugeFixingStats serves the whole loop, as the apps' gaugeStats does.
+template <class G>
+int or_loop(Real *U, lat_index_t *nn, float omega, float precision, int check, int reproject, int max_iter,
+            double *gff, double *theta, int *sweeps, float *ms)
+{
+    const int a = volume() / 2 / NSB, b = 8 * NSB;
+    GaugeFixingStats<4, 3, G, AVERAGE> st(U, HOST_CONSTANTS::SIZE);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0);
+    int done = 0;
+    for (int i = 0; i < max_iter; i++) {
+        G::orStep(a, b, U, nn, 0, omega);
+        G::orStep(a, b, U, nn, 1, omega);
+        if (i % reproject == 0) CommonKernelsSU3::projectSU3(volume() / 32, 32, U, HOST_CONSTANTS::getPtrToDeviceSize());
+        done = i + 1;
+        if (i % check == 0) {
+            st.generateGaugeQuality();
+            if (st.getCurrentA() < precision) break;
+        }
+    }
+    CommonKernelsSU3::projectSU3(volume() / 32, 32, U, HOST_CONSTANTS::getPtrToDeviceSize());
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    cudaEventElapsedTime(ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *gff = st.getCurrentGff();
+    *theta = st.getCurrentA();
+    *sweeps = done;
+    return quality_status();
+}
+
+}  // namespace
+
+extern "C" int refgpu_or_loop(int gauge, Real *U, lat_index_t *nn, float omega, float precision, int check,
+                              int reproject, int max_iter, double *gff, double *theta, int *sweeps, float *ms)
+{
+    if (check < 1 || reproject < 1) return -1;
+    if (gauge == 0) return or_loop<LandauKernelsSU3>(U, nn, omega, precision, check, reproject, max_iter, gff, theta,
+                                                     sweeps, ms);
+    if (gauge == 2) return or_loop<MAGKernelsSU3>(U, nn, omega, precision, check, reproject, max_iter, gff, theta,
+                                                  sweeps, ms);
+    return -1;
+}
+#endif

@@ -35,6 +35,7 @@ _dp = ctypes.POINTER(ctypes.c_double)
 SIGNATURES = {
     "gf_last_error_string": (ctypes.c_char_p, []),
     "gf_version": (ctypes.c_char_p, []),
+    "gf_binary_arch": (_c_int, [ctypes.POINTER(_c_int)]),
     "gf_or_step": (_c_int, [_c_int, _c_int, _vp, _vp, _i32p, _c_int, _c_float, _vp]),
     "gf_micro_step": (_c_int, [_c_int, _c_int, _vp, _vp, _i32p, _c_int, _vp]),
     "gf_sa_step": (_c_int, [_c_int, _c_int, _vp, _vp, _i32p, _c_int, _c_float, _c_int, _c_int, _vp]),

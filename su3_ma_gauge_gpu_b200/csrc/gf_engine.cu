@@ -24,7 +24,9 @@ using namespace gfb;
 struct gf_ctx {
     int gauge = 0, ninst = 0, mixed = 0, device = 0;
     int refine = 0;           // mixed mode 2: FP64 master + FP32 working copy + accumulated W
-    float2 *w = nullptr;      // refine: columns 0, 1 of W of every instance (6 float2 planes of V each)
+    int site_w = 0;           // refine with W in a separate array (Landau, MAG, U1xU1; a Coulomb slice
+                              // keeps its W in its own mu = 0 planes)
+    float2 *w = nullptr;      // site_w: columns 0, 1 of W of every instance (6 float2 planes of V each)
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     std::vector<InstDesc> h_inst;
@@ -39,6 +41,8 @@ struct gf_ctx {
     int trace_cap = 0;
     unsigned int *d_tickets = nullptr;
     int *h_state = nullptr;       // pinned (state, then storage: 2 * ninst)
+    int *h_chunk = nullptr;       // pinned, two slots of 2 * ninst: the states after check chunk k land in
+                                  // slot k & 1 while the host reads slot (k - 1) & 1
     double *h_quality = nullptr;  // pinned
     int *h_sweeps = nullptr;      // pinned (2 * ninst: sweeps, sweeps64)
     void *staging = nullptr;
@@ -167,14 +171,14 @@ int launch_pass(const gf_ctx *c, const EngineDev &e, const PassArgs &a, const gf
 {
     if constexpr (sizeof(R) == 4 && GAUGE != COULOMB && ALGO == ALG_OR) {
         if (sh.variant == 5) {
-            if (c->refine) return launch_site_staged<GAUGE, ALGO, true>(c, e, a, sh.blocks_per_sm);
+            if (c->site_w) return launch_site_staged<GAUGE, ALGO, true>(c, e, a, sh.blocks_per_sm);
             return launch_site_staged<GAUGE, ALGO, false>(c, e, a, sh.blocks_per_sm);
         }
     }
     if constexpr (sizeof(R) == 4 && GAUGE != COULOMB) {
         if (sh.variant == 4 || sh.variant == 5) {  // one thread per site (FP32); 5 = OR-only pipelined
             const unsigned blocks = grid_for(a.c->total_warps * 8, 128);
-            if (c->refine)
+            if (c->site_w)
                 k_batched_pass_site<R, GAUGE, ALGO, true, 2><<<blocks, 128, 0, a.c->stream>>>(
                     e, a.c->total_warps, a.parity, a.p, a.want_state);
             else
@@ -186,13 +190,13 @@ int launch_pass(const gf_ctx *c, const EngineDev &e, const PassArgs &a, const gf
     if constexpr (ALGO == ALG_OR && GAUGE != COULOMB) {
         if (sh.variant == 3) {
             if constexpr (sizeof(R) == 4) {
-                if (c->refine) return launch_rp<R, GAUGE, ALGO, true>(c, e, a, sh.blocks_per_sm);
+                if (c->site_w) return launch_rp<R, GAUGE, ALGO, true>(c, e, a, sh.blocks_per_sm);
             }
             return launch_rp<R, GAUGE, ALGO, false>(c, e, a, sh.blocks_per_sm);
         }
     }
     if constexpr (ALGO == ALG_OR) {
-        if (sh.variant == 1 && !(sizeof(R) == 4 && c->refine)) {
+        if (sh.variant == 1 && !(sizeof(R) == 4 && c->site_w)) {
             switch (sh.warps) {
             case 2: return launch_staged<R, GAUGE, ALGO, 2>(c, e, a, sh.blocks_per_sm);
             case 8: return launch_staged<R, GAUGE, ALGO, 8>(c, e, a, sh.blocks_per_sm);
@@ -202,7 +206,7 @@ int launch_pass(const gf_ctx *c, const EngineDev &e, const PassArgs &a, const gf
     }
     const unsigned blocks = grid_for(a.c->total_warps * 32, 128);
     if constexpr (sizeof(R) == 4) {
-        if (c->refine) {
+        if (c->site_w) {
             if (sh.variant == 2)
                 k_batched_pass<R, GAUGE, ALGO, true, 8><<<blocks, 128, 0, a.c->stream>>>(e, a.c->total_warps,
                                                                                       a.parity, a.p, a.want_state);
@@ -274,11 +278,12 @@ int launch_reunitarise(const gf_ctx *c, int want_state, bool to64)
     const unsigned blocks = grid_for(c->total_links, 256);
     if (c->refine && to64) {
         // refine switch: the FP64 master takes the accumulated W (an exact gauge transformation)
-        k_apply_w<<<blocks, 256, 0, c->stream>>>(c->dev(), c->total_links);
+        if (c->site_w) k_apply_w<<<blocks, 256, 0, c->stream>>>(c->dev(), c->total_links);
+        else k_apply_w_coulomb<false><<<blocks, 256, 0, c->stream>>>(c->dev(), c->total_links);
         c->launches++;
         return launch_status("apply W");
     }
-    if (c->refine && want_state == ST_FP32) {
+    if (c->site_w && want_state == ST_FP32) {
         k_reunitarise_w<<<blocks, 256, 0, c->stream>>>(c->dev(), c->total_links, want_state);
         c->launches++;
         int st = launch_status("reunitarise W");
@@ -318,22 +323,23 @@ int check_ctx(gf_ctx *c)
 }
 
 // One OR check chunk: nsweeps sweeps of the instances sweeping in FP32 (has32) and FP64
-// (has64), an optional reprojection, then the checks: FP64 first, then FP32 with the switch of
-// the instances that crossed switch_theta (so a switched instance is not counted twice).
-int enqueue_or_chunk(gf_ctx *c, int nsweeps, float omega, bool reproject, const CheckParams &base, bool has32,
-                     bool has64)
+// (has64), each followed by a reprojection where reproject_after[k] is set (the drivers reproject
+// right after sweep i when i % reproject == 0, apps/LandauGaugeFixingSU3_4D.cu:249-252), then the
+// checks: FP64 first, then FP32 with the switch of the instances that crossed switch_theta (so a
+// switched instance is not counted twice).
+int enqueue_or_chunk(gf_ctx *c, int nsweeps, float omega, const std::vector<unsigned char> &reproject_after,
+                     const CheckParams &base, bool has32, bool has64)
 {
     int st = GF_OK;
     for (int k = 0; k < nsweeps && !st; k++) {
         if (has32) st = launch_sweep(c, ALG_OR, ST_FP32, omega, 0, 0, 0);
         if (!st && has64) st = launch_sweep(c, ALG_OR, ST_FP64, omega, 0, 0, 0);
+        if (!st && reproject_after[k]) {
+            if (has32) st = launch_reunitarise(c, ST_FP32, false);
+            if (!st && has64) st = launch_reunitarise(c, ST_FP64, false);
+        }
     }
     if (st) return st;
-    if (reproject) {
-        if (has32) st = launch_reunitarise(c, ST_FP32, false);
-        if (!st && has64) st = launch_reunitarise(c, ST_FP64, false);
-        if (st) return st;
-    }
     CheckParams cp = base;
     cp.chunk_sweeps = nsweeps;
     cp.transitions = 1;
@@ -348,10 +354,16 @@ int enqueue_or_chunk(gf_ctx *c, int nsweeps, float omega, bool reproject, const 
             // iterative refinement: instances now in ST_FOLD fold W into the FP64 master, restart
             // the working copy, and are checked on the master (their sweeps are already counted)
             const unsigned blocks = grid_for(c->total_links, 256);
-            k_reunitarise_w<<<blocks, 256, 0, c->stream>>>(c->dev(), c->total_links, ST_FOLD);
-            k_fold_apply<<<blocks, 256, 0, c->stream>>>(c->dev(), c->total_links);
-            k_fold_reset_w<<<blocks, 256, 0, c->stream>>>(c->dev(), c->total_links);
-            c->launches += 3;
+            if (c->site_w) {
+                k_reunitarise_w<<<blocks, 256, 0, c->stream>>>(c->dev(), c->total_links, ST_FOLD);
+                k_fold_apply<<<blocks, 256, 0, c->stream>>>(c->dev(), c->total_links);
+                k_fold_reset_w<<<blocks, 256, 0, c->stream>>>(c->dev(), c->total_links);
+                c->launches += 3;
+            } else {  // Coulomb slices: W32 lives in the working copy's mu = 0 planes
+                k_apply_w_coulomb<true><<<blocks, 256, 0, c->stream>>>(c->dev(), c->total_links);
+                k_fold_coulomb_reset<<<blocks, 256, 0, c->stream>>>(c->dev(), c->total_links);
+                c->launches += 2;
+            }
             if ((st = launch_status("fold"))) return st;
             CheckParams cf = cp;
             cf.want_state = ST_FOLD;
@@ -377,11 +389,6 @@ int gf_create(const gf_ctx_params *p, gf_ctx **out)
         set_error("invalid gf_ctx_params");
         return GF_ERR_INVALID;
     }
-    if (p->mixed == 2 && p->gauge == GF_COULOMB) {
-        // a Coulomb slice already keeps its gauge transformation in its temporal planes
-        set_error("refine mode (mixed = 2) is not available for GF_COULOMB; use mixed = 1");
-        return GF_ERR_UNSUPPORTED;
-    }
     if (p->mixed < 0 || p->mixed > 2) {
         set_error("mixed must be 0, 1 or 2");
         return GF_ERR_INVALID;
@@ -395,6 +402,7 @@ int gf_create(const gf_ctx_params *p, gf_ctx **out)
     c->gauge = p->gauge;
     c->mixed = p->mixed ? 1 : 0;
     c->refine = p->mixed == 2 ? 1 : 0;
+    c->site_w = c->refine && p->gauge != GF_COULOMB;
     cudaGetDevice(&c->device);
     cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device);
     const bool coulomb = p->gauge == GF_COULOMB;
@@ -468,14 +476,14 @@ int gf_create(const gf_ctx_params *p, gf_ctx **out)
     if ((st = cuda_status(cudaMalloc(&c->f64, n64 * sizeof(double2)), "cudaMalloc FP64 field"))) return fail(st);
     if (coulomb && (st = cuda_status(cudaMalloc(&c->t64, (size_t)toff * sizeof(double2)), "cudaMalloc temporal links")))
         return fail(st);
-    if (c->refine && (st = cuda_status(cudaMalloc(&c->w, (size_t)toff * sizeof(float2)), "cudaMalloc W")))
+    if (c->site_w && (st = cuda_status(cudaMalloc(&c->w, (size_t)toff * sizeof(float2)), "cudaMalloc W")))
         return fail(st);
     for (auto &d : c->h_inst) {
         const size_t off = (size_t)reinterpret_cast<uintptr_t>(d.f32);
         d.f32 = c->mixed ? c->f32 + off : nullptr;
         d.f64 = c->f64 + 2 * off;
         if (coulomb) d.t64 = c->t64 + (size_t)reinterpret_cast<uintptr_t>(d.t64);
-        d.w = c->refine ? c->w + (size_t)reinterpret_cast<uintptr_t>(d.w) : nullptr;
+        d.w = c->site_w ? c->w + (size_t)reinterpret_cast<uintptr_t>(d.w) : nullptr;
     }
     const int n = c->ninst;
     if ((st = cuda_status(cudaMalloc(&c->d_inst, sizeof(InstDesc) * n), "cudaMalloc"))) return fail(st);
@@ -495,6 +503,8 @@ int gf_create(const gf_ctx_params *p, gf_ctx **out)
                           "cudaHostAlloc")))
         return fail(st);
     if ((st = cuda_status(cudaHostAlloc(&c->h_sweeps, sizeof(int) * 2 * n, cudaHostAllocDefault), "cudaHostAlloc")))
+        return fail(st);
+    if ((st = cuda_status(cudaHostAlloc(&c->h_chunk, sizeof(int) * 4 * n, cudaHostAllocDefault), "cudaHostAlloc")))
         return fail(st);
     for (int k = 0; k < 2; k++)
         if ((st = cuda_status(cudaEventCreateWithFlags(&c->ev_chunk[k], cudaEventDisableTiming), "cudaEventCreate")))
@@ -535,6 +545,7 @@ int gf_destroy(gf_ctx *c)
     if (c->h_state) cudaFreeHost(c->h_state);
     if (c->h_quality) cudaFreeHost(c->h_quality);
     if (c->h_sweeps) cudaFreeHost(c->h_sweeps);
+    if (c->h_chunk) cudaFreeHost(c->h_chunk);
     for (auto &e : c->ev_chunk)
         if (e) cudaEventDestroy(e);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -587,9 +598,19 @@ int gf_import(gf_ctx *c, int lat, int real, const void *U, int on_host)
         const InstDesc &d = c->h_inst[i];
         const unsigned blocks = grid_for(4 * d.g.V, 256);
         const void *sp = src + (size_t)t * L.slice_reals * es;
-        if (c->refine) {
+        if (c->site_w) {
             if (real == GF_FP64) k_import_refine<double><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (const double *)sp);
             else k_import_refine<float><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (const float *)sp);
+        } else if (c->refine) {
+            // Coulomb slice: FP64 master and FP32 working copy, each with W = 1 in its mu = 0 planes
+            if (real == GF_FP64) {
+                k_import<double, double><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (const double *)sp);
+                k_import<double, float><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (const double *)sp);
+            } else {
+                k_import<float, double><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (const float *)sp);
+                k_import<float, float><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (const float *)sp);
+            }
+            c->launches++;
         } else if (target == ST_FP32) {
             if (real == GF_FP64) k_import<double, float><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (const double *)sp);
             else k_import<float, float><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (const float *)sp);
@@ -639,8 +660,10 @@ int gf_export(gf_ctx *c, int lat, int real, void *U, int on_host)
         const unsigned blocks = grid_for(4 * d.g.V, 256);
         void *dp = dst + (size_t)t * L.slice_reals * es;
         if (c->gauge == GF_COULOMB) {
-            if (real == GF_FP64) k_export_coulomb<double><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (double *)dp);
-            else k_export_coulomb<float><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (float *)dp);
+            if (real == GF_FP64)
+                k_export_coulomb<double><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (double *)dp, c->refine);
+            else
+                k_export_coulomb<float><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (float *)dp, c->refine);
         } else if (c->h_state[c->ninst + i] == 0 && c->refine) {
             if (real == GF_FP64) k_export_refine<double><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (double *)dp);
             else k_export_refine<float><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (float *)dp);
@@ -894,12 +917,15 @@ int gf_fix(gf_ctx *c, const gf_schedule *s, gf_report *rep)
     if ((st = sync_states(c))) return st;
     const int C = s->check_precision;
     struct Variant {
-        int n, repro, has32, has64;
+        int n;
+        std::vector<unsigned char> repro;
+        int has32, has64;
         cudaGraphExec_t exec;
         long long nodes;
     };
     std::vector<Variant> graphs;
-    auto get_graph = [&](int n, int repro, int h32, int h64, cudaGraphExec_t &out) -> int {
+    auto get_graph = [&](int n, const std::vector<unsigned char> &repro, int h32, int h64,
+                         cudaGraphExec_t &out) -> int {
         for (auto &v : graphs)
             if (v.n == n && v.repro == repro && v.has32 == h32 && v.has64 == h64) {
                 out = v.exec;
@@ -925,22 +951,22 @@ int gf_fix(gf_ctx *c, const gf_schedule *s, gf_report *rep)
         out = ex;
         return GF_OK;
     };
-    auto scan = [&](bool &any, bool &h32, bool &h64) {
+    auto scan = [&](const int *states, bool &any, bool &h32, bool &h64) {
         any = h32 = h64 = false;
         for (int i = 0; i < c->ninst; i++) {
-            const int q = c->h_state[i];
+            const int q = states[i];
             any |= q != ST_DONE;
             h32 |= q == ST_FP32;
             h64 |= q == ST_FP64 || q == ST_SWITCH;
         }
     };
     bool any_active, has32, has64;
-    scan(any_active, has32, has64);
+    scan(c->h_state, any_active, has32, has64);
     int issued = 0, launched = 0;
     for (int k = 0; any_active && issued < s->or_max_iter && !st; k++) {
         const int n = k == 0 ? 1 : std::min(C, s->or_max_iter - issued);
-        bool repro = false;
-        for (int i = issued; i < issued + n; i++) repro |= (i % s->reproject) == 0;
+        std::vector<unsigned char> repro(n);
+        for (int k2 = 0; k2 < n; k2++) repro[k2] = ((issued + k2) % s->reproject) == 0;
         if (s->use_graphs) {
             cudaGraphExec_t ex = nullptr;
             if ((st = get_graph(n, repro, has32, has64, ex))) break;
@@ -949,17 +975,18 @@ int gf_fix(gf_ctx *c, const gf_schedule *s, gf_report *rep)
             break;
         }
         issued += n;
-        if ((st = cuda_status(cudaMemcpyAsync(c->h_state, c->d_state, sizeof(int) * 2 * c->ninst,
-                                              cudaMemcpyDeviceToHost, c->stream), "state copy")))
+        if ((st = cuda_status(cudaMemcpyAsync(c->h_chunk + (k & 1) * 2 * c->ninst, c->d_state,
+                                              sizeof(int) * 2 * c->ninst, cudaMemcpyDeviceToHost, c->stream),
+                              "state copy")))
             break;
         if ((st = cuda_status(cudaEventRecord(c->ev_chunk[k & 1], c->stream), "event"))) break;
         launched++;
         if (k >= 1) {
-            // pinned h_state holds the copy of chunk k-1 once its event has fired; the copy of
-            // chunk k lands later and is read in the next iteration
+            // slot (k-1) & 1 holds the complete copy of chunk k-1 once its event has fired; chunk k's
+            // copy lands in the other slot and is read in the next iteration
             if ((st = cuda_status(cudaEventSynchronize(c->ev_chunk[(k - 1) & 1]), "event sync"))) break;
             bool a2, h32b, h64b;
-            scan(a2, h32b, h64b);
+            scan(c->h_chunk + ((k - 1) & 1) * 2 * c->ninst, a2, h32b, h64b);
             any_active = a2;
             has32 = h32b;
             // an instance that switches to FP64 during chunk k is seen here after chunk k+1 was
@@ -1011,7 +1038,7 @@ int gf_autotune(gf_ctx *c, int *choice_fp32, int *choice_fp64)
         const gf_ctx::PassShape *cands = prec == 0 ? cands32 : cands64;
         int ncand = prec == 0 ? 8 : 5;
         if (c->gauge == GF_COULOMB) ncand = 1;
-        else if (prec == 0 && c->refine) ncand = 5;
+        else if (prec == 0 && c->site_w) ncand = 5;
         // scratch field, descriptors and states for this precision
         const InstDesc &last = c->h_inst.back();
         const size_t span32 = (size_t)(reinterpret_cast<const char *>(last.f32 ? last.f32 : (float4 *)nullptr) -
@@ -1041,7 +1068,7 @@ int gf_autotune(gf_ctx *c, int *choice_fp32, int *choice_fp64)
         const void *src = prec == 0 ? (const void *)c->f32 : (const void *)c->f64;
         cudaMemcpyAsync(scratch, src, span, cudaMemcpyDeviceToDevice, c->stream);
         std::vector<InstDesc> hi = c->h_inst;
-        if (prec == 0 && c->refine) {
+        if (prec == 0 && c->site_w) {
             const size_t spanw = (size_t)(last.w - c->w) + (size_t)6 * last.g.V;  // float2 count
             if ((st = cuda_status(cudaMalloc(&wscratch, spanw * sizeof(float2)), "autotune W scratch"))) {
                 cleanup();
@@ -1116,7 +1143,7 @@ int gf_set_pass_shape(gf_ctx *c, int real, int variant, int warps)
 {
     clear_error();
     if (!c || !valid_real(real) || variant < 0 || variant > 5 || (warps != 2 && warps != 4 && warps != 8) ||
-        (variant != 0 && variant != 2 && c->gauge == GF_COULOMB) || (variant == 1 && real == GF_FP32 && c->refine) ||
+        (variant != 0 && variant != 2 && c->gauge == GF_COULOMB) || (variant == 1 && real == GF_FP32 && c->site_w) ||
         ((variant == 2 || variant == 4 || variant == 5) && real == GF_FP64)) {
         set_error("invalid pass shape (Coulomb passes are direct or 64-register; refine-FP32 passes are not "
                   "pipelined; the 64-register and thread-per-site passes are FP32)");

@@ -495,6 +495,123 @@ __global__ void __launch_bounds__(256) k_export_refine(EngineDev e, int i, Rout 
     RefField<Rout>{U, d.g.V}.store18(s, mu, o);
 }
 
+// ---- refine mode for Coulomb timeslices ----------------------------------------------------------
+// A Coulomb slice already keeps its accumulated gauge transformation in its mu = 0 planes (the
+// TRACK_W parity pass), so refine mode needs no separate W array: the FP64 master holds the spatial
+// links and W64, the product of every transformation folded in so far; the FP32 working copy holds
+// its spatial links and W32, the transformation since the last fold.  A fold (and the switch to FP64
+// sweeps) applies W32 exactly to the master:
+//   U64_i(x) <- W32(x) U64_i(x) W32(x + i)^dagger  (i = 1..3, x + i inside the slice),
+//   W64(x)   <- W32(x) W64(x),
+// with every W32 reunitarised in FP64 first, so the master's spatial links stay on their gauge orbit
+// and W64 stays the exact product the export applies to the temporal links.
+__device__ __forceinline__ void mul33(const Link<double> &A, const Link<double> &B, Link<double> &C)
+{
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+            Cx<double> acc = cx<double>(0, 0);
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                const Cx<double> t = cmul(A.e[a][k], B.e[k][b]);
+                acc.x += t.x;
+                acc.y += t.y;
+            }
+            C.e[a][b] = acc;
+        }
+}
+
+// C = A B^dagger
+__device__ __forceinline__ void mul33_adj(const Link<double> &A, const Link<double> &B, Link<double> &C)
+{
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) {
+            Cx<double> acc = cx<double>(0, 0);
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                const Cx<double> t = cmul(A.e[a][k], cx<double>(B.e[b][k].x, -B.e[b][k].y));
+                acc.x += t.x;
+                acc.y += t.y;
+            }
+            C.e[a][b] = acc;
+        }
+}
+
+// W32(s) of a Coulomb slice's working copy, reunitarised in FP64
+__device__ __forceinline__ void coulomb_w32(const InstDesc &d, int64_t s, Link<double> &W)
+{
+    load_link_f64<float>(packed_of<float>(d), s, 0, W);
+    project_rows(W);
+}
+
+// spatial link mu of the master with the working copy's W32 applied: W32(s) U64_mu(s) W32(s + mu)^dagger
+__device__ __forceinline__ void coulomb_apply_w32(const InstDesc &d, int64_t s, int mu, Link<double> &L)
+{
+    const int parity = s >= d.g.Vh;
+    int32_t c[4];
+    site_coords(d.g, s - (parity ? d.g.Vh : 0), parity, c);
+    Link<double> W, Wf, U, M;
+    coulomb_w32(d, s, W);
+    coulomb_w32(d, neighbour_up(d.g, c, mu), Wf);
+    load_link_f64<double>(packed_of<double>(d), s, mu, U);
+    mul33(W, U, M);
+    mul33_adj(M, Wf, L);
+    project_rows(L);
+}
+
+// The fold (FOLD = true: instances in ST_FOLD; the working copy's spatial links restart from the new
+// master) or the switch (ST_SWITCH) of refine Coulomb slices, one thread per link.  The working copy's
+// W32 is reset to 1 by k_fold_coulomb_reset in a separate launch: this one reads W32 of neighbours.
+template <bool FOLD>
+__global__ void __launch_bounds__(256) k_apply_w_coulomb(EngineDev e, int64_t total_links)
+{
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= total_links) return;
+    const int i = find_instance(e.inst, e.ninst, idx, [](const InstDesc &d) { return d.link_begin; });
+    if (e.state[i] != (FOLD ? ST_FOLD : ST_SWITCH)) return;
+    const InstDesc d = e.inst[i];
+    const int64_t l = idx - d.link_begin;
+    const int mu = (int)(l / d.g.V);
+    const int64_t s = l - mu * d.g.V;
+    Link<double> L;
+    if (mu == 0) {
+        Link<double> W, W64;
+        coulomb_w32(d, s, W);
+        load_link_f64<double>(packed_of<double>(d), s, 0, W64);
+        mul33(W, W64, L);
+        project_rows(L);
+    } else {
+        coulomb_apply_w32(d, s, mu, L);
+    }
+    double r[12];
+    pack12(L, r);
+    packed_of<double>(d).store12(s, mu, r);  // each thread reads and writes only its own master link
+    if (FOLD && mu != 0) {
+        float f[12];
+#pragma unroll
+        for (int k = 0; k < 12; k++) f[k] = (float)r[k];
+        packed_of<float>(d).store12(s, mu, f);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_fold_coulomb_reset(EngineDev e, int64_t total_links)
+{
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= total_links) return;
+    const int i = find_instance(e.inst, e.ninst, idx, [](const InstDesc &d) { return d.link_begin; });
+    if (e.state[i] != ST_FOLD) return;
+    const InstDesc d = e.inst[i];
+    const int64_t l = idx - d.link_begin;
+    if (l >= d.g.V) return;  // one thread per site: the mu = 0 planes
+    float one[12];
+#pragma unroll
+    for (int k = 0; k < 12; k++) one[k] = (k == 0 || k == 8) ? 1.f : 0.f;  // rows 0,1 of 1
+    packed_of<float>(d).store12(l, 0, one);
+}
+
 // ---- software-pipelined parity pass --------------------------------------------------------------
 // Same site update as k_batched_pass, but every warp walks a strided list of 8-site tiles and
 // prefetches the 2 links of its lane for tile t+1 into shared memory with cp.async (16-byte,
@@ -924,10 +1041,28 @@ __global__ void __launch_bounds__(256) k_export(EngineDev e, int i, Rout *U)
     RefField<Rout>{U, d.g.V}.store18(s, mu, o);
 }
 
-// Coulomb export of timeslice i: spatial links as k_export; temporal links
+// The accumulated transformation W(s) of Coulomb slice i, from the storage its field lives in; a
+// refine slice whose FP32 working copy is current has W = W32 W64 (working copy after master).
+__device__ __forceinline__ void coulomb_w_total(const EngineDev &e, int i, int64_t s, bool refine, Link<double> &W)
+{
+    const InstDesc d = e.inst[i];
+    if (e.storage[i] == 1) {
+        load_link_f64<double>(packed_of<double>(d), s, 0, W);
+    } else if (!refine) {
+        load_link_f64<float>(packed_of<float>(d), s, 0, W);
+    } else {
+        Link<double> W32, W64;
+        coulomb_w32(d, s, W32);
+        load_link_f64<double>(packed_of<double>(d), s, 0, W64);
+        mul33(W32, W64, W);
+    }
+}
+
+// Coulomb export of timeslice i: spatial links as k_export (a refine slice whose working copy is
+// current exports its master with W32 applied); temporal links
 // U_0(t,x) <- W(t,x) U_0(t,x) W(t+1,x)^dagger, W read from each slice's current storage.
 template <typename Rout>
-__global__ void __launch_bounds__(256) k_export_coulomb(EngineDev e, int i, Rout *U)
+__global__ void __launch_bounds__(256) k_export_coulomb(EngineDev e, int i, Rout *U, int refine)
 {
     const InstDesc d = e.inst[i];
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -938,43 +1073,16 @@ __global__ void __launch_bounds__(256) k_export_coulomb(EngineDev e, int i, Rout
     const bool own64 = e.storage[i] == 1;
     if (mu != 0) {
         if (own64) load_link_f64<double>(packed_of<double>(d), s, mu, L);
+        else if (refine) coulomb_apply_w32(d, s, mu, L);
         else load_link_f64<float>(packed_of<float>(d), s, mu, L);
     } else {
-        const InstDesc dn = e.inst[d.next];
         Link<double> W, Wn, T;
-        if (own64) load_link_f64<double>(packed_of<double>(d), s, 0, W);
-        else load_link_f64<float>(packed_of<float>(d), s, 0, W);
-        if (e.storage[d.next] == 1) load_link_f64<double>(packed_of<double>(dn), s, 0, Wn);
-        else load_link_f64<float>(packed_of<float>(dn), s, 0, Wn);
+        coulomb_w_total(e, i, s, refine != 0, W);
+        coulomb_w_total(e, d.next, s, refine != 0, Wn);
         load_link_f64<double>(PackedField<double>{d.t64, d.g.V}, s, 0, T);
         Link<double> M;  // W T
-#pragma unroll
-        for (int a = 0; a < 3; a++)
-#pragma unroll
-            for (int b = 0; b < 3; b++) {
-                Cx<double> acc = cx<double>(0, 0);
-#pragma unroll
-                for (int k = 0; k < 3; k++) {
-                    const Cx<double> t = cmul(W.e[a][k], T.e[k][b]);
-                    acc.x += t.x;
-                    acc.y += t.y;
-                }
-                M.e[a][b] = acc;
-            }
-#pragma unroll
-        for (int a = 0; a < 2; a++)  // rows 0,1 of M Wn^dagger; row 2 is rebuilt by project_rows
-#pragma unroll
-            for (int b = 0; b < 3; b++) {
-                Cx<double> acc = cx<double>(0, 0);
-#pragma unroll
-                for (int k = 0; k < 3; k++) {
-                    const Cx<double> w = Wn.e[b][k];
-                    const Cx<double> t = cmul(M.e[a][k], cx<double>(w.x, -w.y));
-                    acc.x += t.x;
-                    acc.y += t.y;
-                }
-                L.e[a][b] = acc;
-            }
+        mul33(W, T, M);
+        mul33_adj(M, Wn, L);  // rows 0,1 are what project_rows reads; row 2 is rebuilt there
     }
     project_rows(L);
     Link<Rout> o;

@@ -7,8 +7,6 @@
 // file-scope __device__ array of fixed size instead: GF_NOALLOC_MAX_BLOCKS blocks of 256 sites,
 // i.e. at most 256 * 65536 = 16,777,216 sites (64^4).  Every GPU that loads the library holds
 // this ~1 MiB array until the process exits.
-#include <mutex>
-
 #include "gf_host.hpp"
 #include "gf_kernels.cuh"
 
@@ -26,28 +24,18 @@ struct NoAllocScratch {
 
 static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
 
-// Host code may not use the symbol's host-side name as a device address; the address is
-// looked up once per device, with that device current, and cached.
-static std::mutex g_noalloc_mutex;
-static NoAllocScratch *g_noalloc_ptr[128] = {nullptr};
-
+// Host code may not use the symbol's host-side name as a device address.  The address is looked up
+// on every call, with the caller's device current: the first lookup on a device may load this
+// library's module there (so make that first call before any stream capture), later ones are a
+// table lookup in the runtime.  Nothing is cached across calls, so after a cudaDeviceReset --
+// which unloads the module and places the array anew when it is next loaded -- the next call
+// uses the new address, never one kept from before the reset.
 static int noalloc_scratch(NoAllocScratch **out)
 {
-    int dev = 0;
-    int st = cuda_status(cudaGetDevice(&dev), "cudaGetDevice");
+    void *p = nullptr;
+    const int st = cuda_status(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress");
     if (st) return st;
-    if (dev < 0 || dev >= 128) {
-        set_error("device ordinal %d out of range", dev);
-        return GF_ERR_UNSUPPORTED;
-    }
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_ptr[dev]) {
-        void *p = nullptr;
-        st = cuda_status(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress");
-        if (st) return st;
-        g_noalloc_ptr[dev] = static_cast<NoAllocScratch *>(p);
-    }
-    *out = g_noalloc_ptr[dev];
+    *out = static_cast<NoAllocScratch *>(p);
     return GF_OK;
 }
 

@@ -167,7 +167,21 @@ struct gf_stats {
 extern "C" {
 
 const char *gf_last_error_string(void) { return gfb::g_err; }
-const char *gf_version(void) { return "su3_ma_gauge_gpu_b200 0.1 (sm_100a)"; }
+const char *gf_version(void) { return "su3_ma_gauge_gpu_b200 0.2 (sm_100a)"; }
+
+int gf_binary_arch(int *arch)
+{
+    clear_error();
+    if (!arch) {
+        set_error("NULL argument");
+        return GF_ERR_INVALID;
+    }
+    cudaFuncAttributes a{};
+    const int st = cuda_status(cudaFuncGetAttributes(&a, k_set_hot_ref<double>), "cudaFuncGetAttributes");
+    if (st) return st;
+    *arch = a.binaryVersion;
+    return GF_OK;
+}
 
 int gf_or_step(int gauge, int real, void *U, void *Udw, const int32_t size[4], int parity, float or_parameter,
                void *stream)

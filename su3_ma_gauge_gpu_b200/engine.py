@@ -110,7 +110,8 @@ class GaugeFixer:
     def __init__(self, sizes, gauge="landau", mixed=True, stream=None):
         """mixed: False (FP64 only), True (FP32 storage, then FP64), or "refine" (FP64 master,
         FP32 working copy with the accumulated gauge transformation W applied to the master at
-        the switch: the FP32 phase never moves the field off its gauge orbit)."""
+        the switch: the FP32 phase never moves the field off its gauge orbit; for Coulomb the W of a
+        timeslice is the one it keeps in its temporal planes)."""
         self.sizes = [tuple(int(v) for v in s) for s in sizes]
         self.gauge = GAUGES[gauge] if isinstance(gauge, str) else int(gauge)
         arr = (ctypes.c_int32 * (4 * len(self.sizes)))(*[v for s in self.sizes for v in s])

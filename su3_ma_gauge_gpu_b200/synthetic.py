@@ -164,15 +164,34 @@ def _torch_linalg(size, eps: float, seed: int, transform: bool, device: str):
     return links, f0
 
 
-def smooth_config(size, eps: float, seed: int, transform: bool = True, dtype=np.float64, device=None):
+def _to_gpupattern_torch(links, size, dtype):
+    """to_gpupattern on the device: complex [4, V, 3, 3] tensor -> GpuPattern tensor of V*72 reals."""
+    import torch
+
+    V = volume(size)
+    split = torch.from_numpy(lexicographic_to_split(size)).to(links.device)
+    tdt = torch.float64 if np.dtype(dtype) == np.float64 else torch.float32
+    arr = torch.empty((4, 3, 3, 2, V), dtype=tdt, device=links.device)
+    arr[:, :, :, 0, :][..., split] = links.real.permute(0, 2, 3, 1).to(tdt)
+    arr[:, :, :, 1, :][..., split] = links.imag.permute(0, 2, 3, 1).to(tdt)
+    return arr.reshape(-1)
+
+
+def smooth_config(size, eps: float, seed: int, transform: bool = True, dtype=np.float64, device=None,
+                  as_tensor: bool = False):
     """The "known fixed point" input: exp(i*eps*H) links under a seeded Haar gauge transform.
 
     Returns (field in GpuPattern layout, functional of the untransformed field).  With
     device="cuda" the eigen/QR work runs on the GPU (for large lattices); the returned field
-    is a host numpy array either way.
+    is a host numpy array, or with as_tensor=True a tensor left on that device (the layout
+    conversion then runs there too, which matters at 48^4 where the complex links are 3 GB).
     """
     if device is not None:
         links, f0 = _torch_linalg(size, eps, seed, transform, device)
+        if as_tensor:
+            U = _to_gpupattern_torch(links, size, dtype)
+            del links
+            return U, f0
         return to_gpupattern(links.cpu().numpy(), size, dtype), f0
     rng = np.random.default_rng(seed)
     links = smooth_links(size, eps, rng)

@@ -138,6 +138,55 @@ def ref_set_hot(size, seed, counter, dtype=np.float64):
     return U
 
 
+# ---- the reference's own CUDA kernels (oracle/_ref/libref_gpu_*.so, built by oracle/Makefile) -----
+def refgpu(name: str):
+    """Load oracle/_ref/<name> (the reference's kernels for one compile-time extent and precision,
+    behind oracle/ref_gpu.cu's C entry points), or None if it was not built."""
+    p = REF_DIR / name
+    if not p.exists():
+        return None
+    lib = ctypes.CDLL(str(p))
+    lib.refgpu_step.argtypes = [ctypes.c_int, ctypes.c_int, _P, _P, _P, ctypes.c_int, ctypes.c_float, ctypes.c_int,
+                                ctypes.c_int]
+    lib.refgpu_quality.argtypes = [ctypes.c_int, _P, ctypes.POINTER(ctypes.c_double),
+                                   ctypes.POINTER(ctypes.c_double)]
+    lib.refgpu_project.argtypes = [ctypes.c_int, _P]
+    if hasattr(lib, "refgpu_or_loop"):
+        lib.refgpu_or_loop.argtypes = [ctypes.c_int, _P, _P, ctypes.c_float, ctypes.c_float, ctypes.c_int,
+                                       ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                       ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int),
+                                       ctypes.POINTER(ctypes.c_float)]
+    return lib
+
+
+def refgpu_config(lib):
+    size = (ctypes.c_int * 4)()
+    es = lib.refgpu_config(size)
+    return tuple(size), es
+
+
+def refgpu_neighbours(lib, size, timeslice=False) -> np.ndarray:
+    """The reference's neighbour table (host array of int32) for the library's extents."""
+    V = volume(size) if not timeslice else volume(size[1:])
+    nn = np.zeros(8 * V, np.int32)
+    lib.refgpu_neighbour_table(int(timeslice), nn.ctypes.data_as(_P))
+    return nn
+
+
+def refgpu_or_loop(lib, gauge, U_ptr, nn_ptr, omega=1.7, precision=1e-12, check=20, reproject=100,
+                   max_iter=20000):
+    """The apps' overrelaxation loop (apps/LandauGaugeFixingSU3_4D.cu:244-271) on the reference's
+    kernels, in place on the device array at U_ptr; precision is passed as a float, as the apps
+    hold it.  Returns (functional, theta, sweeps, milliseconds) of the last check."""
+    g, a = ctypes.c_double(), ctypes.c_double()
+    n, ms = ctypes.c_int(), ctypes.c_float()
+    rc = lib.refgpu_or_loop(gauge, U_ptr, nn_ptr, ctypes.c_float(omega), ctypes.c_float(precision), check, reproject,
+                            max_iter, ctypes.byref(g), ctypes.byref(a), ctypes.byref(n), ctypes.byref(ms))
+    if rc != 0:
+        raise RuntimeError(f"refgpu_or_loop failed: {rc}")
+    return g.value, a.value, n.value, ms.value
+
+
 # ---- layout helpers (reference GpuPattern) -----------------------------------------------------
 def links(U, size):
     """GpuPattern array -> complex array [mu][V][3][3]."""

@@ -2,7 +2,6 @@
 argument validation works without touching the GPU (no compute calls here)."""
 import ctypes
 import re
-import subprocess
 from pathlib import Path
 
 import pytest
@@ -35,13 +34,20 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_library_is_built_for_sm100a():
+    """The build passes exactly the sm_100a target to nvcc (the runtime answer is checked on the
+    GPU by test_device_code_runs_as_sm100a)."""
+    from su3_ma_gauge_gpu_b200 import build
+
+    assert build.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+@pytest.mark.gpu
+def test_device_code_runs_as_sm100a(cuda):
     from su3_ma_gauge_gpu_b200 import _lib
 
-    out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf", str(_lib.LIB_PATH)],
-                         capture_output=True, text=True)
-    if out.returncode != 0:
-        pytest.skip("cuobjdump unavailable")
-    assert "sm_100a" in out.stdout
+    arch = ctypes.c_int()
+    _lib.check(_lib.lib().gf_binary_arch(ctypes.byref(arch)), "gf_binary_arch")
+    assert arch.value == 100
 
 
 def test_validation_without_gpu():
@@ -72,9 +78,10 @@ def test_context_parameter_checks_without_gpu():
     L = _lib.lib()
     sizes = (ctypes.c_int32 * 4)(4, 4, 4, 4)
     h = ctypes.c_void_p()
-    p = _lib.CtxParams(gauge=_lib.GF_COULOMB, ninstances=1, sizes=sizes, mixed=2, stream=None)
-    assert L.gf_create(ctypes.byref(p), ctypes.byref(h)) == _lib.GF_ERR_UNSUPPORTED
-    assert b"refine" in L.gf_last_error_string()
+    odd_t = (ctypes.c_int32 * 4)(3, 4, 4, 4)
+    p = _lib.CtxParams(gauge=_lib.GF_COULOMB, ninstances=1, sizes=odd_t, mixed=2, stream=None)
+    assert L.gf_create(ctypes.byref(p), ctypes.byref(h)) == _lib.GF_ERR_INVALID
+    assert b"Nt = 3" in L.gf_last_error_string()
     p = _lib.CtxParams(gauge=_lib.GF_LANDAU, ninstances=1, sizes=sizes, mixed=3, stream=None)
     assert L.gf_create(ctypes.byref(p), ctypes.byref(h)) == _lib.GF_ERR_INVALID
     p = _lib.CtxParams(gauge=_lib.GF_LANDAU, ninstances=0, sizes=sizes, mixed=0, stream=None)

@@ -135,6 +135,36 @@ def test_fix_fp64_matches_oracle_driver(cuda):
     assert np.abs(out - ref).max() < 1e-9
 
 
+@pytest.mark.parametrize("reproject,check", [(7, 10), (3, 10), (30, 20)])
+def test_fix_reprojection_cadence_matches_oracle_driver(cuda, reproject, check):
+    """The drivers reproject right after sweep i whenever i % reproject == 0
+    (apps/LandauGaugeFixingSU3_4D.cu:249-252), also when reproject is smaller than, or not a multiple
+    of, checkprecision: gf_fix (plain FP64) reproduces the oracle driver's field to 1e-12 per
+    link after a fixed number of sweeps, and its sweep count and functional at convergence."""
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer
+
+    size = (4, 4, 4, 8)
+    U, _ = S.smooth_config(size, 0.3, 33)
+    for max_iter, prec in ((47, 1e-30), (3000, 1e-11)):
+        sch = _sched(precision=prec, check_precision=check, reproject=reproject, or_max_iter=max_iter)
+        with GaugeFixer([size], mixed=False) as gf:
+            gf.load(0, U)
+            rep = gf.fix(sch)[0]
+            out = np.zeros_like(U)
+            gf.store(0, out)
+        ref = U.copy()
+        osch = O.Schedule(0, 0, 0.01, 0.4, 0, sch.or_max_iter, 1.7, sch.precision, sch.check_precision,
+                          sch.reproject, 1)
+        r, _ = O.fix(ref, size, O.LANDAU, osch)
+        assert rep.or_sweeps == r.or_iterations
+        if max_iter < 100:  # budget spent: this run also checks after its last, partial chunk
+            assert np.abs(out - ref).max() < 1e-12
+        else:
+            assert rep.converged
+            assert rep.gff == pytest.approx(r.gff, rel=1e-12)
+            assert np.abs(out - ref).max() < 1e-9
+
+
 def _mixed_vs_fp64(size, eps, seed):
     from su3_ma_gauge_gpu_b200.engine import GaugeFixer
 
@@ -323,6 +353,85 @@ def test_coulomb_fix_every_slice(cuda):
         gq, aq = O.quality(out[t * Vs * 72:(t + 1) * Vs * 72].copy(), (1,) + size[1:], O.COULOMB)
         assert aq < 1e-11
         assert gq == pytest.approx(reps[t].gff, rel=1e-9)
+
+
+@pytest.mark.parametrize("fold", [0, 1], ids=["fp64-polish", "iterative-refinement"])
+def test_coulomb_refine_lands_on_the_fp64_maximum(cuda, fold):
+    """Refine mode for Coulomb timeslices: each slice's FP32 working copy tracks its gauge
+    transformation in its temporal planes, and the folds / the switch apply it exactly to the FP64
+    master.  Every slice reaches theta < 1e-12 with a functional equal to the plain-FP64 batched fix
+    (which test_coulomb_batched_matches_sequential_timeslices pins to the reference's slice-by-slice
+    flow) to 1e-10 relative, and the exported field (temporal links W(t) U_0 W(t+1)^dagger) has the
+    oracle's Coulomb quality of that functional."""
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer
+
+    size = (4, 8, 8, 8)
+    Vs = int(np.prod(size[1:]))
+    U = np.concatenate([S.smooth_config((1,) + size[1:], 0.3, 180 + t)[0] for t in range(size[0])])
+    sch = _sched(precision=1e-12, switch_theta=1e-9, check_precision=10, or_max_iter=6000, fold=fold)
+    reps, outs = {}, {}
+    for mode in (False, "refine"):
+        with GaugeFixer([size], gauge="coulomb", mixed=mode) as gf:
+            gf.load(0, U)
+            reps[mode] = gf.fix(sch)
+            outs[mode] = np.zeros_like(U)
+            gf.store(0, outs[mode])
+    for t in range(size[0]):
+        r, f = reps["refine"][t], reps[False][t]
+        assert r.converged and r.theta < 1e-12
+        assert r.or_sweeps_fp64 < r.or_sweeps
+        assert r.gff == pytest.approx(f.gff, rel=1e-10), t
+        gq, aq = O.quality(outs["refine"][t * Vs * 72:(t + 1) * Vs * 72].copy(), (1,) + size[1:], O.COULOMB)
+        assert gq == pytest.approx(f.gff, rel=1e-10)
+        assert aq < 1e-11
+    # the temporal links of both exports agree: the same per-slice transformations were applied
+    a = outs["refine"].reshape(size[0], 4, 3, 3, 2, Vs)[:, 0]
+    b = outs[False].reshape(size[0], 4, 3, 3, 2, Vs)[:, 0]
+    assert np.abs(a - b).max() < 1e-5
+
+
+def test_coulomb_refine_export_is_gauge_equivalent(cuda):
+    """A refine Coulomb context exported mid-run (working copy current, W32 not yet folded) is a gauge
+    transform of its input: every plaquette, spatial and temporal, is unchanged to FP64 rounding."""
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer
+
+    size = (4, 4, 6, 4)
+    Vs = int(np.prod(size[1:]))
+    U = np.concatenate([S.smooth_config((1,) + size[1:], 0.3, 190 + t)[0] for t in range(size[0])])
+    with GaugeFixer([size], gauge="coulomb", mixed="refine") as gf:
+        gf.load(0, U)
+        gf.sweeps("or", 25, 1.7)
+        out = np.zeros_like(U)
+        gf.store(0, out)
+    full_in = S.from_gpupattern(_timeslices_to_gpupattern(U, size), size)
+    full_out = S.from_gpupattern(_timeslices_to_gpupattern(out, size), size)
+    assert np.abs(_plaquettes(full_out, size) - _plaquettes(full_in, size)).max() < 1e-12
+    assert np.abs(out - U).max() > 1e-3
+
+
+def _timeslices_to_gpupattern(T, size):
+    """Inverse of synthetic.gpupattern_to_timeslices (for the plaquette check)."""
+    nt, nx, ny, nz = size
+    vs, v = nx * ny * nz, nt * nx * ny * nz
+    t, x, y, z = (a.reshape(-1) for a in np.meshgrid(np.arange(nt), np.arange(nx), np.arange(ny), np.arange(nz),
+                                                     indexing="ij"))
+    l = ((t * nx + x) * ny + y) * nz + z
+    s_full = l // 2 + ((t + x + y + z) % 2) * (v // 2)
+    s_slice = ((x * ny + y) * nz + z) // 2 + ((x + y + z) % 2) * (vs // 2)
+    src = np.asarray(T).reshape(nt, 72, vs)
+    out = np.empty((72, v), dtype=src.dtype)
+    out[:, s_full] = src[t, :, s_slice].T
+    return out.reshape(-1)
+
+
+def _plaquettes(L, size):
+    vals = []
+    for mu in range(4):
+        for nu in range(mu + 1, 4):
+            fm, fn = S.forward_neighbour_lex(size, mu), S.forward_neighbour_lex(size, nu)
+            P = np.einsum("nij,njk,nlk,nml->nim", L[mu], L[nu][fm], L[mu][fn].conj(), L[nu].conj())
+            vals.append(np.trace(P, axis1=1, axis2=2).real)
+    return np.array(vals)
 
 
 def _mag_app_temperatures(sa_steps, sa_min, sa_max, lo, hi, factor):

@@ -34,28 +34,18 @@ REF = O.REF_DIR
 
 
 def _reflib(name):
-    p = REF / name
-    if not p.exists():
-        pytest.skip(f"{p.name} not built (reference tree absent when oracle/ was built)")
-    lib = ctypes.CDLL(str(p))
-    lib.refgpu_step.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
-                                ctypes.c_int, ctypes.c_float, ctypes.c_int, ctypes.c_int]
-    lib.refgpu_quality.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
-                                   ctypes.POINTER(ctypes.c_double)]
+    lib = O.refgpu(name)
+    if lib is None:
+        pytest.skip(f"{name} not built (reference tree absent when oracle/ was built)")
     return lib
 
 
 def _config(lib):
-    size = (ctypes.c_int * 4)()
-    es = lib.refgpu_config(size)
-    return tuple(size), es
+    return O.refgpu_config(lib)
 
 
 def _nn(torch, lib, size, timeslice):
-    V = int(np.prod(size)) if not timeslice else int(np.prod(size[1:]))
-    nn = np.zeros(8 * V, np.int32)
-    lib.refgpu_neighbour_table(timeslice, nn.ctypes.data_as(ctypes.c_void_p))
-    return torch.from_numpy(nn).cuda()
+    return torch.from_numpy(O.refgpu_neighbours(lib, size, timeslice)).cuda()
 
 
 def _ours(torch, gauge, algo, U, Udw, size, real, param, seed, counter):
@@ -161,6 +151,103 @@ def test_quality_matches_reference_stats(cuda, gauge, prec):
     rel = 1e-12 if prec == "f64" else 1e-5
     assert st.getCurrentGff() == pytest.approx(g.value, rel=rel)
     assert st.getCurrentA() == pytest.approx(a.value, rel=rel if prec == "f64" else 1e-4)
+
+
+SIZE32 = (32, 32, 32, 32)
+
+
+@pytest.fixture(scope="module")
+def landau32_input():
+    """The headline input: 32^4, U = exp(i 0.3 H) under a seeded Haar gauge transform (FP64
+    GpuPattern), generated on the GPU."""
+    return S.smooth_config(SIZE32, 0.3, 1234, device="cuda")
+
+
+def test_landau_32x4_fix_matches_reference_path(cuda, landau32_input):
+    """The headline workload end to end.  The seeded 32^4 input is fixed (1) by the reference's own
+    FP64 kernels driven by the Landau app's overrelaxation loop (apps/LandauGaugeFixingSU3_4D.cu:
+    244-271: orStep pair, projectSU3 at i % 100 == 0, check at i % 20 == 0, closing projectSU3),
+    (2) by this library's gf_fix in refine mixed precision with the bench's schedule, and (3) by
+    gf_fix in plain FP64.  All three reach theta < 1e-12 and the final FP64 functionals agree to
+    1e-10 relative."""
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer, Schedule
+
+    torch = cuda
+    lib = _reflib("libref_gpu_X32T32_f64.so")
+    U, _ = landau32_input
+    dU = torch.from_numpy(U.copy()).cuda()
+    nn = _nn(torch, lib, SIZE32, 0)
+    F_ref, th_ref, n_ref, ms_ref = O.refgpu_or_loop(lib, 0, dU.data_ptr(), nn.data_ptr())
+    del dU, nn
+    torch.cuda.empty_cache()
+    dIn = torch.from_numpy(U).cuda()
+    stream = torch.cuda.Stream()
+    sched = Schedule(or_max_iter=20000, precision=1e-12, switch_theta=1e-9, check_precision=20, reproject=100,
+                     micro_updates=0)
+    res = {}
+    for mode in ("refine", False):
+        with GaugeFixer([SIZE32], mixed=mode, stream=stream) as gf:
+            gf.load(0, dIn)
+            res[mode] = gf.fix(sched)[0]
+    print(json.dumps({"reference": {"F": F_ref, "theta": th_ref, "sweeps": n_ref, "ms": ms_ref},
+                      **{str(m): {"F": r.gff, "theta": r.theta, "sweeps": r.or_sweeps, "fp64_sweeps": r.or_sweeps_fp64,
+                                  "F_rel_err": abs(r.gff - F_ref) / F_ref} for m, r in res.items()}}))
+    assert th_ref < 1e-12
+    for mode, r in res.items():
+        assert r.converged and r.theta < 1e-12, mode
+        assert abs(r.gff - F_ref) / F_ref < 1e-10, (mode, r.gff, F_ref)
+    # plain FP64 follows the reference's trajectory: it crosses 1e-12 at the same check or the next
+    assert abs(res[False].or_sweeps - n_ref) <= 20
+
+
+def test_landau_32x4_fp32_sweeps_match_reference_kernels(cuda, landau32_input):
+    """Per-sweep FP32 link fields at the headline size: three OR sweeps of the 32^4 input by the
+    reference's FP32 kernels (built with -use_fast_math, as its Makefile does) and by this library
+    -- the plugin pass in place on the GpuPattern array; the engine's FP32 storage; and refine
+    mode's FP32 working copy, exported as W U64 W^dagger of its FP64 master -- agree within 1e-5
+    max-abs on the stored rows after every sweep."""
+    from su3_ma_gauge_gpu_b200 import _lib
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer
+
+    torch = cuda
+    lib = _reflib("libref_gpu_X32T32_f32.so")
+    U, _ = landau32_input
+    U32 = U.astype(np.float32)
+    nn = _nn(torch, lib, SIZE32, 0)
+    rU = torch.from_numpy(U32.copy()).cuda()
+    pU = torch.from_numpy(U32.copy()).cuda()
+    out = torch.empty_like(rU)
+    L = _lib.lib()
+    s = _lib.size_arg(SIZE32)
+    stream = torch.cuda.Stream()
+    fast = GaugeFixer([SIZE32], mixed=True, stream=stream)
+    fast.load(0, rU)
+    refine = GaugeFixer([SIZE32], mixed="refine", stream=stream)
+    refine.load(0, torch.from_numpy(U).cuda())
+    errs = []
+    try:
+        for k in range(3):
+            for p in (0, 1):
+                assert lib.refgpu_step(0, 0, rU.data_ptr(), None, nn.data_ptr(), p, 1.7, 0, 0) == 0
+                _lib.check(L.gf_or_step(0, 0, pU.data_ptr(), None, s, p, ctypes.c_float(1.7), None), "gf_or_step")
+            fast.sweeps("or", 1, 1.7)
+            refine.sweeps("or", 1, 1.7)
+            torch.cuda.synchronize()
+            ref = rU.cpu().numpy()
+            e = {"plugin": O.rows01_maxdiff(ref, pU.cpu().numpy(), SIZE32)}
+            for name, gf in (("engine_fp32", fast), ("engine_refine", refine)):
+                gf.store(0, out)
+                torch.cuda.synchronize()
+                e[name] = O.rows01_maxdiff(ref, out.cpu().numpy(), SIZE32)
+            errs.append(e)
+    finally:
+        fast.close()
+        refine.close()
+    print(json.dumps(errs))
+    assert O.rows01_maxdiff(rU.cpu().numpy(), U32, SIZE32) > 1e-3  # the sweeps moved the field
+    for e in errs:
+        for name, v in e.items():
+            assert v < 1e-5, (name, v)
 
 
 def test_reference_kernel_timing(cuda):
