@@ -56,6 +56,10 @@ def pass_kernel_name(code: int, real: str, refine: bool) -> str:
         return f"k_batched_pass_site<{r}, LANDAU, OR{w}> (one thread per site)"
     if code == 33:
         return f"k_batched_pass_site_staged<LANDAU, OR{w}> (one thread per site, cp.async pipelined)"
+    if code == 16:
+        return f"k_batched_pass_pair<{r}, LANDAU, OR{w}> (two lanes per site)"
+    if code == 116:
+        return f"k_batched_pass_pair_rp<{r}, LANDAU, OR{w}> (two lanes per site, register prefetch, persistent)"
     if code == 64:
         return f"k_batched_pass<{r}, LANDAU, OR{w}> (64 registers)"
     if code in (2, 4, 8):

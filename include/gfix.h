@@ -157,7 +157,7 @@ typedef struct gf_ctx_params {
  * that drive the per-copy loop, plus the mixed-precision switch */
 typedef struct gf_schedule {
     int random_trafo;      /* randomtrafo: random gauge transformation first */
-    uint32_t seed;         /* seed (Philox key word 1; instance i uses seed + i) */
+    uint32_t seed;         /* seed (Philox key word 1; see rng_streams) */
     uint32_t rng_counter;  /* first Philox launch counter (PhiloxWrapper::getNextCounter) */
     int sa_steps;          /* sasteps */
     float sa_min, sa_max;  /* samin, samax */
@@ -198,6 +198,14 @@ typedef struct gf_schedule {
                               copy leaves a rounding-noise floor of about 1e-12 in the master's
                               theta that only FP64 sweeps remove (they do so within ~20 sweeps);
                               0: fold until theta < precision or the folds stall */
+    int rng_streams;       /* Philox streams of the instances: 0 = instance i draws key word seed + i
+                              (independent streams, the same launch counters); 1 = the reference
+                              apps' one stream (lattice/rng/PhiloxWrapper.hxx:90,142-145): every
+                              instance draws key word seed, instance i starting after the counters
+                              instances 0 .. i-1 would have used fixed one after the other (random
+                              trafo and SA; not with sr_max_iter > 0) -- for a Coulomb lattice the
+                              timeslices then draw exactly what apps/CoulombGaugeFixingSU3_4D.cu
+                              draws for them */
 } gf_schedule;
 
 typedef struct gf_report {
@@ -236,15 +244,17 @@ int gf_fix(gf_ctx *ctx, const gf_schedule *schedule, gf_report *reports);
 /* Autotuner: times the candidate launch shapes of the OR parity pass (one warp per 8-site tile;
  * the same capped at 64 registers (FP32); persistent with the next tile prefetched into
  * registers; FP32 with one thread per site; pipelined with cp.async prefetch and 2, 4 or 8 warps
- * per block) on a scratch copy of the field (and of W in refine contexts) and keeps the fastest
- * per precision.  Outputs: 0 = direct, 64 = direct with 64 registers, 100 = register prefetch,
- * 32 = thread per site, 33 = thread per site pipelined with cp.async, 2/4/8 = warps per block of
- * the pipelined pass (-1: precision not used). */
+ * per block; two lanes per site, direct and persistent with register prefetch) on a scratch copy of
+ * the field (and of W in refine contexts) and keeps the fastest per precision.  Outputs: 0 = direct,
+ * 64 = direct with 64 registers, 100 = register prefetch, 32 = thread per site, 33 = thread per site
+ * pipelined with cp.async, 2/4/8 = warps per block of the pipelined pass, 16 = two lanes per site,
+ * 116 = two lanes per site with register prefetch (-1: precision not used). */
 int gf_autotune(gf_ctx *ctx, int *choice_fp32, int *choice_fp64);
 /* Fix the launch shape instead: variant 0 (direct), 1 (pipelined, warps = 2, 4 or 8), 2 (FP32
- * direct capped at 64 registers), 3 (register prefetch), 4 (FP32, one thread per site) or 5 (FP32,
- * one thread per site pipelined; OR, the other rules run as 4).  GF_COULOMB: 0 or 2; refine FP32:
- * not 1. */
+ * direct capped at 64 registers), 3 (register prefetch), 4 (FP32, one thread per site), 5 (FP32,
+ * one thread per site pipelined; OR, the other rules run as 4), 6 (two lanes per site) or 7 (two
+ * lanes per site with register prefetch; OR, the other rules run as 6).  GF_COULOMB: 0 or 2;
+ * refine FP32: not 1. */
 int gf_set_pass_shape(gf_ctx *ctx, int real, int variant, int warps);
 /* Number of instances (lattices, or timeslices for GF_COULOMB). */
 int gf_instances(gf_ctx *ctx);

@@ -100,6 +100,58 @@ void orc_fix_f64(double *U, const int32_t size[4], int gauge, const orc_schedule
 void orc_fix_f32(float *U, const int32_t size[4], int gauge, const orc_schedule *sched,
                  uint32_t *counter, orc_result *res, int nthreads);
 
+/* Whole-run driver of one gauge copy as the apps run it, for every gauge:
+ *   apps/LandauGaugeFixingSU3_4D.cu:185-271 (and U1xU1), apps/MAGaugeFixingSU3_4D.cu:197-333,
+ *   the per-slice body of apps/CoulombGaugeFixingSU3_4D.cu:216-301 --
+ * random gauge transformation; simulated annealing, either the Landau/Coulomb apps' for-loop over
+ * sa_steps linearly falling temperatures (sa_mode 0) or the MAG/U1xU1 apps' do-while whose step is
+ * divided by sa_slow_factor while the temperature lies in [sa_slow_lo, sa_slow_hi] (sa_mode 2),
+ * each temperature running sa_repeat SA sweeps, each followed by micro_updates microcanonical
+ * sweeps, with a reprojection at every temperature index i with i % reproject == 0; stochastic
+ * relaxation (MAG) until theta < precision or theta < sr_stop_theta, checked at i % checkprecision
+ * == 0; overrelaxation with the same check and reprojection cadence; the closing projectSU3.
+ * For ORC_COULOMB, U is the slice-t array and Udw the slice-(t-1) array (size = {1, Nx, Ny, Nz});
+ * both are reprojected, as the Coulomb app does.  *counter is the host Philox counter
+ * (PhiloxWrapper::getNextCounter), advanced as the apps advance it. */
+typedef struct orc_app_schedule {
+    int random_trafo;
+    int sa_steps;
+    float sa_min, sa_max;
+    int micro_updates;
+    int sa_mode;            /* 0: for-loop, linear (Landau, Coulomb); 2: do-while with slowed window */
+    int sa_repeat;          /* SA (+ micro) sweeps per temperature (MAG app: 5) */
+    double sa_slow_lo, sa_slow_hi;
+    float sa_slow_factor;
+    int sr_max_iter;
+    float sr_parameter;
+    double sr_stop_theta;   /* MAG app: 1e-6 */
+    int or_max_iter;
+    float or_parameter;
+    float precision;
+    int check_precision;
+    int reproject;
+    uint32_t seed;
+} orc_app_schedule;
+
+typedef struct orc_app_result {
+    double gff, theta;      /* last quality computed (OR loop, or SR loop if OR never checked) */
+    int or_iterations, sa_sweeps, sr_iterations;
+} orc_app_result;
+
+void orc_fix_app_f64(double *U, double *Udw, const int32_t size[4], int gauge, const orc_app_schedule *sched,
+                     uint32_t *counter, orc_app_result *res, int nthreads);
+void orc_fix_app_f32(float *U, float *Udw, const int32_t size[4], int gauge, const orc_app_schedule *sched,
+                     uint32_t *counter, orc_app_result *res, int nthreads);
+
+/* The Coulomb app's slice loop (apps/CoulombGaugeFixingSU3_4D.cu:199-311) for one gauge copy:
+ * timeslices t = 0 .. Nt-1 one after the other, each fixed by orc_fix_app with UtUp = slice t
+ * and UtDw = slice t-1 (periodic) of the GpuPatternTimeslice array U (slice t at offset
+ * 72 * Vs * t), the Philox counter running on from slice to slice.  res has Nt entries. */
+void orc_fix_coulomb_f64(double *U, const int32_t size[4], const orc_app_schedule *sched, uint32_t *counter,
+                         orc_app_result *res, int nthreads);
+void orc_fix_coulomb_f32(float *U, const int32_t size[4], const orc_app_schedule *sched, uint32_t *counter,
+                         orc_app_result *res, int nthreads);
+
 #ifdef __cplusplus
 }
 #endif

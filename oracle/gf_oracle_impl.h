@@ -639,6 +639,91 @@ void FN(orc_fix)(REAL *U, const int32_t size[4], int gauge, const orc_schedule *
     res->or_iterations = it;
 }
 
+/* orc_fix_app: see gf_oracle.h.  The loops follow apps/LandauGaugeFixingSU3_4D.cu:204-271 (sa_mode 0,
+ * also the Coulomb app's slice body, apps/CoulombGaugeFixingSU3_4D.cu:216-301) and
+ * apps/MAGaugeFixingSU3_4D.cu:222-333 (sa_mode 2 and the SR loop). */
+void FN(orc_fix_app)(REAL *U, REAL *Udw, const int32_t size[4], int gauge, const orc_app_schedule *sc,
+                     uint32_t *counter, orc_app_result *res, int nthreads)
+{
+    const int coulomb = gauge == ORC_COULOMB;
+    REAL *dw = coulomb ? Udw : U;
+    double gff = 0, theta = 0;
+    int sa_done = 0;
+#define ORC_PROJECT()                                               \
+    do {                                                            \
+        FN(orc_project)(U, size, nthreads);                         \
+        if (coulomb) FN(orc_project)(Udw, size, nthreads);          \
+    } while (0)
+    if (sc->random_trafo) {
+        FN(orc_step)(U, dw, size, gauge, ORC_RANDOM, 0, 0.f, sc->seed, (*counter)++, nthreads);
+        FN(orc_step)(U, dw, size, gauge, ORC_RANDOM, 1, 0.f, sc->seed, (*counter)++, nthreads);
+    }
+    const int repeat = sc->sa_repeat > 0 ? sc->sa_repeat : 1;
+    float temperature = sc->sa_max;
+    const float base = sc->sa_steps > 0 ? (sc->sa_max - sc->sa_min) / (float)sc->sa_steps : 0.f;
+    int i = 0;
+    for (;;) {
+        if (sc->sa_steps <= 0) break;
+        if (sc->sa_mode != 2 && i >= sc->sa_steps) break;
+        float step = base;
+        if (sc->sa_mode == 2 && (double)temperature <= sc->sa_slow_hi && (double)temperature >= sc->sa_slow_lo)
+            step = base / sc->sa_slow_factor;
+        for (int r = 0; r < repeat; r++) {
+            FN(orc_step)(U, dw, size, gauge, ORC_SA, 0, temperature, sc->seed, (*counter)++, nthreads);
+            FN(orc_step)(U, dw, size, gauge, ORC_SA, 1, temperature, sc->seed, (*counter)++, nthreads);
+            sa_done++;
+            for (int m = 0; m < sc->micro_updates; m++) {
+                FN(orc_step)(U, dw, size, gauge, ORC_MICRO, 0, 0.f, 0, 0, nthreads);
+                FN(orc_step)(U, dw, size, gauge, ORC_MICRO, 1, 0.f, 0, 0, nthreads);
+            }
+        }
+        if (i % sc->reproject == 0) ORC_PROJECT();
+        temperature -= step;
+        i++;
+        if (sc->sa_mode == 2 && !(temperature >= sc->sa_min)) break;
+    }
+    int sr = 0;
+    for (int k = 0; k < sc->sr_max_iter; k++) {
+        FN(orc_step)(U, dw, size, gauge, ORC_SR, 0, sc->sr_parameter, sc->seed, (*counter)++, nthreads);
+        FN(orc_step)(U, dw, size, gauge, ORC_SR, 1, sc->sr_parameter, sc->seed, (*counter)++, nthreads);
+        sr = k + 1;
+        if (k % sc->reproject == 0) ORC_PROJECT();
+        if (k % sc->check_precision == 0) {
+            FN(orc_quality)(U, size, gauge, 0, &gff, &theta, 0, 0, nthreads);
+            if (theta < sc->precision || theta < sc->sr_stop_theta) break;
+        }
+    }
+    int it = 0;
+    for (int k = 0; k < sc->or_max_iter; k++) {
+        FN(orc_step)(U, dw, size, gauge, ORC_OR, 0, sc->or_parameter, 0, 0, nthreads);
+        FN(orc_step)(U, dw, size, gauge, ORC_OR, 1, sc->or_parameter, 0, 0, nthreads);
+        it = k + 1;
+        if (k % sc->reproject == 0) ORC_PROJECT();
+        if (k % sc->check_precision == 0) {
+            FN(orc_quality)(U, size, gauge, 0, &gff, &theta, 0, 0, nthreads);
+            if (theta < sc->precision) break;
+        }
+    }
+    ORC_PROJECT();
+#undef ORC_PROJECT
+    res->gff = gff;
+    res->theta = theta;
+    res->or_iterations = it;
+    res->sa_sweeps = sa_done;
+    res->sr_iterations = sr;
+}
+
+void FN(orc_fix_coulomb)(REAL *U, const int32_t size[4], const orc_app_schedule *sc, uint32_t *counter,
+                         orc_app_result *res, int nthreads)
+{
+    const int32_t ss[4] = {1, size[1], size[2], size[3]};
+    const int64_t slice = (int64_t)72 * size[1] * size[2] * size[3];
+    for (int t = 0; t < size[0]; t++) {
+        const int tdw = t > 0 ? t - 1 : size[0] - 1;
+        FN(orc_fix_app)(U + slice * t, U + slice * tdw, ss, ORC_COULOMB, sc, counter, &res[t], nthreads);
+    }
+}
+
 #undef CPX
 #undef MAT
 #undef RNG

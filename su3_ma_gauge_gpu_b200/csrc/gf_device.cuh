@@ -201,7 +201,23 @@ struct AlgoParams {
     float param;      // OR omega, SA temperature, SR probability
     uint32_t seed;
     uint32_t counter;
+    uint32_t counter_stride;  // batches: 0 = instance i draws key word seed + i; > 0 = every instance draws
+                              // key word seed, instance i from launch counter counter + i * counter_stride
 };
+
+// Philox key word and launch counter of instance i of a batch.  By default every instance has a
+// stream of its own (key word seed + i, the same counters).  With counter_stride > 0 the instances
+// continue one stream, as the reference apps do when they fix gauge copies or timeslices one after
+// the other (PhiloxWrapper::getNextCounter is one process-wide counter, lattice/rng/PhiloxWrapper.hxx:
+// 90,142-145): key word seed, instance i starting counter_stride launches after instance i - 1.
+__host__ __device__ __forceinline__ uint32_t inst_seed(const AlgoParams &p, int i)
+{
+    return p.counter_stride ? p.seed : p.seed + (uint32_t)i;
+}
+__host__ __device__ __forceinline__ uint32_t inst_counter(const AlgoParams &p, int i)
+{
+    return p.counter + (uint32_t)i * p.counter_stride;
+}
 
 // OrUpdate::calculateUpdate (OrUpdate.hxx:66-75)
 template <typename R>
@@ -491,6 +507,43 @@ __device__ __forceinline__ void subgroup_step_site(Link<R> (&up)[4], Link<R> (&d
         left_mult_dcolumn<I, J>((*wcols)[0], w, 0);
         left_mult_dcolumn<I, J>((*wcols)[1], w, 1);
     }
+}
+
+// Two lanes per site: lane `role` (0 or 1; its partner is lane ^ 16) holds directions 2*role and
+// 2*role + 1, each as its up link U_mu(x) and down link U_mu(x - mu).  The quaternion sum is
+// (v0 + v1) + (v2 + v3) -- the additions of the 4-lane butterfly, in the same order -- and both
+// lanes compute the same g.  Each lane then updates its four links, and with SITE_W column `role`
+// of the site's D = W - 1, so no lane repeats another's work except the SU(2) update itself.
+template <int GAUGE, int ALGO, int I, int J, typename R, bool SITE_W>
+__device__ __forceinline__ void subgroup_step_pair(Link<R> (&up)[2], Link<R> (&dn)[2], int role, const AlgoParams &p,
+                                                   Rng<R> &rng, Cx<R> (*wcol)[3])
+{
+    R a[4], b[4], w[4];
+    subgroup_contrib<GAUGE, I, J>(up[0], dn[0], 2 * role, a);
+    subgroup_contrib<GAUGE, I, J>(up[1], dn[1], 2 * role + 1, b);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const bool zero = (GAUGE == U1XU1 && (k == 1 || k == 2)) || (GAUGE == MAG && k == 3);
+        const R v = a[k] + b[k];
+        w[k] = zero ? (R)0 : v + __shfl_xor_sync(0xffffffffu, v, 16);
+    }
+    subgroup_finish<GAUGE, ALGO>(w, p, rng);
+    const R h[4] = {w[0], -w[1], -w[2], -w[3]};
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        left_mult<I, J>(up[j], w);
+        right_mult<I, J>(dn[j], h);
+    }
+    if (SITE_W) left_mult_dcolumn<I, J>(*wcol, w, role);
+}
+
+template <int GAUGE, int ALGO, typename R, bool SITE_W = false>
+__device__ __forceinline__ void site_update_pair(Link<R> (&up)[2], Link<R> (&dn)[2], int role, const AlgoParams &p,
+                                                 Rng<R> &rng, Cx<R> (*wcol)[3] = nullptr)
+{
+    subgroup_step_pair<GAUGE, ALGO, 0, 2, R, SITE_W>(up, dn, role, p, rng, wcol);
+    subgroup_step_pair<GAUGE, ALGO, 1, 2, R, SITE_W>(up, dn, role, p, rng, wcol);
+    subgroup_step_pair<GAUGE, ALGO, 0, 1, R, SITE_W>(up, dn, role, p, rng, wcol);
 }
 
 // the three subgroups in the reference order (0,2), (1,2), (0,1) (SU3::perSubgroup, SU3.hxx:762-771);

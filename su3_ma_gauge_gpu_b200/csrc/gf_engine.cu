@@ -50,6 +50,7 @@ struct gf_ctx {
     cudaEvent_t ev_chunk[2] = {nullptr, nullptr};
     mutable long long launches = 0;  // kernels this context has launched (graph nodes per replay)
     int num_sms = 148;
+    uint32_t counter_stride = 0;  // Philox streams of the batch (AlgoParams::counter_stride), set by gf_fix
     // parity-pass launch shape per precision ([0] FP32, [1] FP64): variant 0 = one warp per
     // 8-site tile, 128 threads per block; variant 1 = pipelined (cp.async prefetch of the next
     // tile), `warps` warps per block, grid = num_sms * blocks_per_sm
@@ -166,9 +167,54 @@ int launch_site_staged(const gf_ctx *c, const EngineDev &e, const PassArgs &a, i
     return launch_status("batched parity pass (thread per site, pipelined)");
 }
 
+template <typename R, int GAUGE, int ALGO, bool SITE_W>
+int launch_pair_rp(const gf_ctx *c, const EngineDev &e, const PassArgs &a, int blocks_per_sm)
+{
+    auto kern = k_batched_pass_pair_rp<R, GAUGE, ALGO, SITE_W>;
+    static int occ_cached = 0;  // resident blocks per SM of this instantiation
+    int occ = blocks_per_sm;
+    if (occ <= 0) {
+        if (occ_cached <= 0) {
+            int o = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, 128, 0) != cudaSuccess || o < 1) o = 1;
+            occ_cached = o;
+        }
+        occ = occ_cached;
+    }
+    const int64_t need = ((a.c->total_warps + 1) / 2 + 3) / 4;  // 16-site pair tiles, 4 warps per block
+    const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)c->num_sms * occ));
+    kern<<<blocks, 128, 0, a.c->stream>>>(e, a.c->total_warps, a.parity, a.p, a.want_state);
+    return launch_status("batched parity pass (two lanes per site, register prefetch)");
+}
+
 template <typename R, int GAUGE, int ALGO>
 int launch_pass(const gf_ctx *c, const EngineDev &e, const PassArgs &a, const gf_ctx::PassShape &sh)
 {
+    if constexpr (GAUGE != COULOMB) {
+        // two lanes per site: 7 = persistent with register prefetch (OR), 6 = direct (every rule,
+        // and the other rules when 7 is chosen)
+        if constexpr (ALGO == ALG_OR && sizeof(R) == 4) {  // FP64 would spill at 255 registers
+            if (sh.variant == 7) {
+                if (c->site_w) return launch_pair_rp<R, GAUGE, ALGO, true>(c, e, a, sh.blocks_per_sm);
+                return launch_pair_rp<R, GAUGE, ALGO, false>(c, e, a, sh.blocks_per_sm);
+            }
+        }
+        if (sh.variant == 6 || sh.variant == 7) {
+            const unsigned blocks = grid_for((a.c->total_warps + 1) / 2 * 32, 128);
+            if constexpr (sizeof(R) == 4) {
+                if (c->site_w)
+                    k_batched_pass_pair<R, GAUGE, ALGO, true, 4><<<blocks, 128, 0, a.c->stream>>>(
+                        e, a.c->total_warps, a.parity, a.p, a.want_state);
+                else
+                    k_batched_pass_pair<R, GAUGE, ALGO, false, 4><<<blocks, 128, 0, a.c->stream>>>(
+                        e, a.c->total_warps, a.parity, a.p, a.want_state);
+            } else {
+                k_batched_pass_pair<R, GAUGE, ALGO, false, 2><<<blocks, 128, 0, a.c->stream>>>(
+                    e, a.c->total_warps, a.parity, a.p, a.want_state);
+            }
+            return launch_status("batched parity pass (two lanes per site)");
+        }
+    }
     if constexpr (sizeof(R) == 4 && GAUGE != COULOMB && ALGO == ALG_OR) {
         if (sh.variant == 5) {
             if (c->site_w) return launch_site_staged<GAUGE, ALGO, true>(c, e, a, sh.blocks_per_sm);
@@ -239,7 +285,8 @@ int launch_sweep_on(const gf_ctx *c, const EngineDev &e, const gf_ctx::PassShape
                     float param, uint32_t seed, uint32_t counter_even, uint32_t counter_odd)
 {
     for (int parity = 0; parity < 2; parity++) {
-        PassArgs a{c, parity, AlgoParams{param, seed, parity ? counter_odd : counter_even}, want_state};
+        PassArgs a{c, parity, AlgoParams{param, seed, parity ? counter_odd : counter_even, c->counter_stride},
+                   want_state};
         int st = dispatch_gauge_algo<BatchedPass>(c->gauge, algo, a, e, shape);
         if (st) return st;
         c->launches++;
@@ -801,6 +848,50 @@ int gf_fix(gf_ctx *c, const gf_schedule *s, gf_report *rep)
     if (s->autotune && (!c->tuned[1] || (c->mixed && !c->tuned[0])) && (st = gf_autotune(c, nullptr, nullptr)))
         return st;
     uint32_t ctr = s->rng_counter;
+    // the SA temperatures.  sa_mode 0: the Landau/Coulomb apps' linear schedule
+    // (apps/LandauGaugeFixingSU3_4D.cu:212-234); 1: geometric; 2: the MAG / U1xU1 apps' do-while, step
+    // (max-min)/steps divided by sa_slow_factor inside [sa_slow_lo, sa_slow_hi] (the float temperature
+    // compared with the double bounds, apps/MAGaugeFixingSU3_4D.cu:233-266).
+    std::vector<float> temps;
+    const int mode = s->sa_mode ? s->sa_mode : (s->sa_geometric ? 1 : 0);
+    if (s->sa_steps > 0 && mode == 2) {
+        float T = s->sa_max;
+        const float base_step = (s->sa_max - s->sa_min) / (float)s->sa_steps;
+        const float slow = s->sa_slow_factor > 0 ? s->sa_slow_factor : 1.f;
+        do {
+            const float step = ((double)T <= s->sa_slow_hi && (double)T >= s->sa_slow_lo) ? base_step / slow : base_step;
+            temps.push_back(T);
+            T -= step;
+        } while (T >= s->sa_min && (int)temps.size() < 100 * s->sa_steps);
+    } else if (s->sa_steps > 0) {
+        float T = s->sa_max;
+        const float dT = (s->sa_max - s->sa_min) / (float)s->sa_steps;
+        const double ratio = s->sa_steps > 1 ? pow((double)s->sa_min / s->sa_max, 1.0 / (s->sa_steps - 1)) : 1.0;
+        for (int i = 0; i < s->sa_steps; i++) {
+            temps.push_back(mode == 1 ? (float)(s->sa_max * pow(ratio, (double)i)) : T);
+            T -= dT;
+        }
+    }
+    // Philox streams: rng_streams = 1 continues one stream through the instances, the way the apps
+    // fix copies / timeslices one after the other -- instance i starts where instance i - 1's
+    // random trafo and SA sweeps (two launch counters each) end.  That count must be known before
+    // the run, so SR (whose length depends on convergence) is excluded.
+    struct StreamGuard {
+        gf_ctx *c;
+        ~StreamGuard() { c->counter_stride = 0; }
+    } stream_guard{c};
+    if (s->rng_streams == 1) {
+        if (s->sr_max_iter > 0) {
+            set_error("rng_streams = 1 needs a schedule without SR (its length depends on convergence)");
+            return GF_ERR_INVALID;
+        }
+        const int repeat_ = s->sa_repeat > 0 ? s->sa_repeat : 1;
+        c->counter_stride = (uint32_t)(2 * (s->random_trafo ? 1 : 0) + 2 * repeat_ * (int)temps.size());
+        if (c->counter_stride == 0) c->counter_stride = 1;  // nothing random: any non-zero stride
+    } else if (s->rng_streams != 0) {
+        set_error("rng_streams must be 0 or 1");
+        return GF_ERR_INVALID;
+    }
     // the precisions the instances sweep in before the OR phase (set by gf_import)
     if ((st = sync_states(c))) return st;
     bool pre32, pre64;
@@ -813,11 +904,8 @@ int gf_fix(gf_ctx *c, const gf_schedule *s, gf_report *rep)
         if ((st = gf_sweeps(c, ALG_RANDOM, 1, 0.f, (int)s->seed, (int)ctr))) return st;
         ctr += 2;
     }
-    // simulated annealing with microcanonical steps.  sa_mode 0: the Landau/Coulomb apps' linear
-    // schedule (apps/LandauGaugeFixingSU3_4D.cu:212-234); 1: geometric; 2: the MAG / U1xU1 apps'
-    // do-while, step (max-min)/steps divided by sa_slow_factor inside [sa_slow_lo, sa_slow_hi]
-    // (apps/MAGaugeFixingSU3_4D.cu:233-266).  Every temperature runs sa_repeat SA sweeps, each
-    // followed (every micro_every-th) by micro_updates microcanonical sweeps.
+    // simulated annealing with microcanonical steps: every temperature runs sa_repeat SA sweeps,
+    // each followed (every micro_every-th) by micro_updates microcanonical sweeps.
     int sa_done = 0;
     const int every = s->micro_every > 0 ? s->micro_every : 1;
     const int repeat = s->sa_repeat > 0 ? s->sa_repeat : 1;
@@ -834,28 +922,8 @@ int gf_fix(gf_ctx *c, const gf_schedule *s, gf_report *rep)
         if (i % s->reproject == 0) return gf_reunitarize(c);
         return GF_OK;
     };
-    const int mode = s->sa_mode ? s->sa_mode : (s->sa_geometric ? 1 : 0);
-    if (s->sa_steps > 0 && mode == 2) {
-        float T = s->sa_max;
-        const float base_step = (s->sa_max - s->sa_min) / (float)s->sa_steps;
-        const float slow = s->sa_slow_factor > 0 ? s->sa_slow_factor : 1.f;
-        int i = 0;
-        do {
-            const float step = ((double)T <= s->sa_slow_hi && (double)T >= s->sa_slow_lo) ? base_step / slow : base_step;
-            if ((st = sa_temperature(T, i))) return st;
-            T -= step;
-            i++;
-        } while (T >= s->sa_min && i < 100 * s->sa_steps);
-    } else if (s->sa_steps > 0) {
-        float T = s->sa_max;
-        const float dT = (s->sa_max - s->sa_min) / (float)s->sa_steps;
-        const double ratio = s->sa_steps > 1 ? pow((double)s->sa_min / s->sa_max, 1.0 / (s->sa_steps - 1)) : 1.0;
-        for (int i = 0; i < s->sa_steps; i++) {
-            const float Ti = mode == 1 ? (float)(s->sa_max * pow(ratio, (double)i)) : T;
-            if ((st = sa_temperature(Ti, i))) return st;
-            T -= dT;
-        }
-    }
+    for (size_t i = 0; i < temps.size(); i++)
+        if ((st = sa_temperature(temps[i], (int)i))) return st;
     // stochastic relaxation (the MAG app, apps/MAGaugeFixingSU3_4D.cu:278-297): SR sweeps until
     // every instance has theta < max(precision, sr_stop_theta), checked every checkprecision sweeps
     int sr_done = 0;
@@ -1027,18 +1095,19 @@ int gf_autotune(gf_ctx *c, int *choice_fp32, int *choice_fp64)
     clear_error();
     int st = check_ctx(c);
     if (st) return st;
-    // direct; register prefetch (persistent); pipelined with 2, 4, 8 warps per block; (FP32 only)
-    // direct capped at 64 registers and one thread per site (plain and pipelined).  Coulomb passes
-    // are direct only; refine-FP32 passes (W tracking) are not the 4-lane pipelined one.
-    static const gf_ctx::PassShape cands64[] = {{0, 4, 0}, {3, 4, 0}, {1, 2, 0}, {1, 4, 0}, {1, 8, 0}};
+    // direct; register prefetch (persistent); two lanes per site (direct, and persistent with register
+    // prefetch); pipelined with 2, 4, 8 warps per block; (FP32 only) direct capped at 64 registers and
+    // one thread per site (plain and pipelined).  Coulomb passes are direct only; refine-FP32 passes
+    // (W tracking) are not the 4-lane pipelined one.
+    static const gf_ctx::PassShape cands64[] = {{0, 4, 0}, {3, 4, 0}, {6, 4, 0}, {1, 2, 0}, {1, 4, 0}, {1, 8, 0}};
     static const gf_ctx::PassShape cands32[] = {{0, 4, 0}, {2, 4, 0}, {3, 4, 0}, {4, 4, 0}, {5, 4, 0},
-                                                {1, 2, 0}, {1, 4, 0}, {1, 8, 0}};
+                                                {6, 4, 0}, {7, 4, 0}, {1, 2, 0}, {1, 4, 0}, {1, 8, 0}};
     for (int prec = 0; prec < 2; prec++) {
         if (prec == 0 && !c->mixed) continue;
         const gf_ctx::PassShape *cands = prec == 0 ? cands32 : cands64;
-        int ncand = prec == 0 ? 8 : 5;
+        int ncand = prec == 0 ? 10 : 6;
         if (c->gauge == GF_COULOMB) ncand = 1;
-        else if (prec == 0 && c->site_w) ncand = 5;
+        else if (prec == 0 && c->site_w) ncand = 7;
         // scratch field, descriptors and states for this precision
         const InstDesc &last = c->h_inst.back();
         const size_t span32 = (size_t)(reinterpret_cast<const char *>(last.f32 ? last.f32 : (float4 *)nullptr) -
@@ -1128,6 +1197,8 @@ int gf_autotune(gf_ctx *c, int *choice_fp32, int *choice_fp64)
                : sh.variant == 3 ? 100
                : sh.variant == 4 ? 32
                : sh.variant == 5 ? 33
+               : sh.variant == 6 ? 16
+               : sh.variant == 7 ? 116
                                  : 0;
     };
     if (choice_fp32) *choice_fp32 = c->mixed ? code(c->shape[0]) : -1;
@@ -1137,12 +1208,13 @@ int gf_autotune(gf_ctx *c, int *choice_fp32, int *choice_fp64)
 
 // Set the parity-pass launch shape by hand: variant 0 (one warp per tile), 1 (pipelined with
 // `warps` = 2, 4 or 8 warps per block), 2 (FP32 direct capped at 64 registers), 3 (register
-// prefetch, persistent), 4 (FP32, one thread per site) or 5 (the same, pipelined with cp.async;
-// OR only, other update rules fall back to variant 4).
+// prefetch, persistent), 4 (FP32, one thread per site), 5 (the same, pipelined with cp.async;
+// OR only, other update rules fall back to variant 4), 6 (two lanes per site) or 7 (two lanes per
+// site, persistent with register prefetch; FP32 OR only, the other cases run as 6).
 int gf_set_pass_shape(gf_ctx *c, int real, int variant, int warps)
 {
     clear_error();
-    if (!c || !valid_real(real) || variant < 0 || variant > 5 || (warps != 2 && warps != 4 && warps != 8) ||
+    if (!c || !valid_real(real) || variant < 0 || variant > 7 || (warps != 2 && warps != 4 && warps != 8) ||
         (variant != 0 && variant != 2 && c->gauge == GF_COULOMB) || (variant == 1 && real == GF_FP32 && c->site_w) ||
         ((variant == 2 || variant == 4 || variant == 5) && real == GF_FP64)) {
         set_error("invalid pass shape (Coulomb passes are direct or 64-register; refine-FP32 passes are not "

@@ -84,7 +84,8 @@ __global__ void __launch_bounds__(128, MINB) k_batched_pass(EngineDev e, int64_t
     const InstDesc d = e.inst[i];
     const PackedField<R> f = packed_of<R>(d);
     AlgoParams pi = p;
-    pi.seed = p.seed + (uint32_t)i;
+    pi.seed = inst_seed(p, i);
+    pi.counter = inst_counter(p, i);
     parity_pass_warp<R, GAUGE, ALGO, PackedField<R>, GAUGE == COULOMB, SITE_W>(f, f, d.g, warp - d.warp_begin, parity,
                                                                                pi, d.w);
 }
@@ -203,7 +204,7 @@ __global__ void __launch_bounds__(128) k_batched_pass_rp(EngineDev e, int64_t to
             reconstruct(dn);
             Rng<R> rng;
             if (ALGO == ALG_SA || ALGO == ALG_SR || ALGO == ALG_RANDOM)
-                rng.init(ref_rng_tid(cur.h), p.seed + (uint32_t)cur.inst, p.counter);
+                rng.init(ref_rng_tid(cur.h), inst_seed(p, cur.inst), inst_counter(p, cur.inst));
             Cx<R> wcol[3];
             if (SITE_W) {
 #pragma unroll
@@ -274,7 +275,7 @@ __global__ void __launch_bounds__(128, MINB) k_batched_pass_site(EngineDev e, in
         reconstruct(dn[mu]);
     }
     Rng<R> rng;
-    if (ALGO == ALG_SA || ALGO == ALG_SR || ALGO == ALG_RANDOM) rng.init(ref_rng_tid(h), p.seed + (uint32_t)i, p.counter);
+    if (ALGO == ALG_SA || ALGO == ALG_SR || ALGO == ALG_RANDOM) rng.init(ref_rng_tid(h), inst_seed(p, i), inst_counter(p, i));
     site_update_thread<GAUGE, ALGO, R, SITE_W>(up, dn, p, rng, &wc);
 #pragma unroll
     for (int mu = 0; mu < 4; mu++) {
@@ -287,6 +288,195 @@ __global__ void __launch_bounds__(128, MINB) k_batched_pass_site(EngineDev e, in
 #pragma unroll
             for (int r = 0; r < 3; r++)
                 d.w[(int64_t)(k * 3 + r) * d.g.V + s] = make_float2((float)wc[k][r].x, (float)wc[k][r].y);
+    }
+}
+
+// ---- two lanes per site --------------------------------------------------------------------------
+// A warp updates 16 sites: lanes 0-7 and 16-23 the sites of 8-site tile 2T, lanes 8-15 and 24-31
+// those of tile 2T + 1.  Lane `role` = lane >> 4 of a site holds directions 2 role and 2 role + 1
+// (their up links at x and down links at x - mu), so a site's 8 links are in 2 lanes instead of 4:
+// half the shuffles, the SU(2) update computed twice per site instead of four times, and each of
+// the two tracked columns of W updated by one lane.  A tile's two lanes of a site are lane and
+// lane ^ 16, always in the same tile, so an idle tile (past the end, or an instance in another
+// state) only ever exchanges with itself.  Not for COULOMB (its slices carry W in a link slot).
+struct PairSite {
+    int inst;           // -1: idle
+    int64_t h, s, sd[2];
+};
+
+__device__ __forceinline__ PairSite pair_site(const InstDesc &d, int i, int64_t tile, int parity)
+{
+    const int lane = threadIdx.x & 31, role = lane >> 4;
+    PairSite ps;
+    ps.inst = i;
+    ps.h = (tile - d.warp_begin) * 8 + (lane & 7);
+    int32_t c[4];
+    site_coords(d.g, ps.h, parity, c);
+    ps.s = ps.h + (parity ? d.g.Vh : 0);
+#pragma unroll
+    for (int j = 0; j < 2; j++) ps.sd[j] = neighbour_down(d.g, c, 2 * role + j);
+    return ps;
+}
+
+template <typename R, int GAUGE, int ALGO, bool SITE_W, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_batched_pass_pair(EngineDev e, int64_t total_tiles, int parity,
+                                                                 AlgoParams p, int want_state)
+{
+    static_assert(GAUGE != COULOMB, "Coulomb slices use k_batched_pass");
+    const int lane = threadIdx.x & 31, role = lane >> 4;
+    const int64_t tile = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 2 + ((lane >> 3) & 1);
+    int i = -1;
+    if (tile < total_tiles) {
+        i = find_instance(e.inst, e.ninst, tile, [](const InstDesc &d) { return d.warp_begin; });
+        if (e.state[i] != want_state) i = -1;
+    }
+    if (!__any_sync(0xffffffffu, i >= 0)) return;
+    Link<R> up[2], dn[2];
+    Cx<R> wcol[3];
+    PairSite ps{-1, 0, 0, {0, 0}};
+    PackedField<R> f{nullptr, 0};
+    float2 *W = nullptr;
+    if (i >= 0) {
+        const InstDesc &d = e.inst[i];
+        ps = pair_site(d, i, tile, parity);
+        f = packed_of<R>(d);
+        W = d.w;
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            load_link<R>(f, ps.s, 2 * role + j, up[j]);
+            load_link<R>(f, ps.sd[j], 2 * role + j, dn[j]);
+        }
+        if (SITE_W) {
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+                const float2 v = W[(int64_t)(role * 3 + r) * f.V + ps.s];
+                wcol[r] = cx<R>((R)v.x, (R)v.y);
+            }
+        }
+    } else {  // idle tile: no coupling, so every update leaves the (unstored) links alone
+#pragma unroll
+        for (int j = 0; j < 2; j++)
+#pragma unroll
+            for (int a = 0; a < 3; a++)
+#pragma unroll
+                for (int b = 0; b < 3; b++) up[j].e[a][b] = dn[j].e[a][b] = cx<R>((R)0, (R)0);
+#pragma unroll
+        for (int r = 0; r < 3; r++) wcol[r] = cx<R>((R)0, (R)0);
+    }
+    Rng<R> rng;
+    if (ALGO == ALG_SA || ALGO == ALG_SR || ALGO == ALG_RANDOM)
+        rng.init(ref_rng_tid(ps.h), inst_seed(p, i < 0 ? 0 : i), inst_counter(p, i < 0 ? 0 : i));
+    site_update_pair<GAUGE, ALGO, R, SITE_W>(up, dn, role, p, rng, &wcol);
+    if (i < 0) return;
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        store_link<R>(f, ps.s, 2 * role + j, up[j]);
+        store_link<R>(f, ps.sd[j], 2 * role + j, dn[j]);
+    }
+    if (SITE_W) {
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+            W[(int64_t)(role * 3 + r) * f.V + ps.s] = make_float2((float)wcol[r].x, (float)wcol[r].y);
+    }
+}
+
+// Persistent form with register prefetch: each warp walks a strided list of 16-site pair tiles and
+// loads the next one's links (and W column) into registers before it updates the current one.
+template <typename R>
+struct PairRegs {
+    PairSite ps;
+    R up[2][12], dn[2][12];
+    float2 w[3];
+};
+
+template <typename R, bool SITE_W>
+__device__ __forceinline__ void fetch_pair_regs(const EngineDev &e, const InstCache &ic, int64_t tile,
+                                                int64_t total_tiles, int parity, int want_state, PairRegs<R> &t)
+{
+    t.ps.inst = -1;
+    if (tile >= total_tiles) return;
+    int i;
+    if (e.ninst <= kInstCache) {
+        i = find_instance(ic.d, ic.n, tile, [](const InstDesc &d) { return d.warp_begin; });
+        if (ic.state[i] != want_state) return;
+    } else {
+        i = find_instance(e.inst, e.ninst, tile, [](const InstDesc &d) { return d.warp_begin; });
+        if (e.state[i] != want_state) return;
+    }
+    const InstDesc &d = inst_at(e, ic, i);
+    const int role = (threadIdx.x & 31) >> 4;
+    t.ps = pair_site(d, i, tile, parity);
+    const PackedField<R> f = packed_of<R>(d);
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        f.load12(t.ps.s, 2 * role + j, t.up[j]);
+        f.load12(t.ps.sd[j], 2 * role + j, t.dn[j]);
+    }
+    if (SITE_W) {
+#pragma unroll
+        for (int r = 0; r < 3; r++) t.w[r] = d.w[(int64_t)(role * 3 + r) * d.g.V + t.ps.s];
+    }
+}
+
+template <typename R, int GAUGE, int ALGO, bool SITE_W>
+__global__ void __launch_bounds__(128) k_batched_pass_pair_rp(EngineDev e, int64_t total_tiles, int parity,
+                                                              AlgoParams p, int want_state)
+{
+    static_assert(GAUGE != COULOMB, "Coulomb slices use k_batched_pass");
+    __shared__ InstCache ic;
+    fill_inst_cache(e, ic);
+    const int lane = threadIdx.x & 31, role = lane >> 4, half = (lane >> 3) & 1;
+    const int64_t npair = (total_tiles + 1) / 2;                 // 16-site pair tiles
+    const int64_t stride = (int64_t)gridDim.x * 4;
+    int64_t pt = (int64_t)blockIdx.x * 4 + (threadIdx.x >> 5);   // this warp's pair tile
+    PairRegs<R> cur;
+    fetch_pair_regs<R, SITE_W>(e, ic, pt * 2 + half, total_tiles, parity, want_state, cur);
+    // every lane of a warp runs the same iterations (pt is warp-uniform), so the shuffles are safe
+    for (; pt < npair; pt += stride) {
+        PairRegs<R> nxt;
+        fetch_pair_regs<R, SITE_W>(e, ic, (pt + stride) * 2 + half, total_tiles, parity, want_state, nxt);
+        const int i = cur.ps.inst;
+        if (__any_sync(0xffffffffu, i >= 0)) {
+            Link<R> up[2], dn[2];
+            Cx<R> wcol[3];
+#pragma unroll
+            for (int j = 0; j < 2; j++) {
+                if (i >= 0) {
+                    unpack12(up[j], cur.up[j]);
+                    reconstruct(up[j]);
+                    unpack12(dn[j], cur.dn[j]);
+                    reconstruct(dn[j]);
+                } else {
+#pragma unroll
+                    for (int a = 0; a < 3; a++)
+#pragma unroll
+                        for (int b = 0; b < 3; b++) up[j].e[a][b] = dn[j].e[a][b] = cx<R>((R)0, (R)0);
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+                wcol[r] = (SITE_W && i >= 0) ? cx<R>((R)cur.w[r].x, (R)cur.w[r].y) : cx<R>((R)0, (R)0);
+            Rng<R> rng;
+            if (ALGO == ALG_SA || ALGO == ALG_SR || ALGO == ALG_RANDOM)
+                rng.init(ref_rng_tid(cur.ps.h), inst_seed(p, i < 0 ? 0 : i), inst_counter(p, i < 0 ? 0 : i));
+            site_update_pair<GAUGE, ALGO, R, SITE_W>(up, dn, role, p, rng, &wcol);
+            if (i >= 0) {
+                const InstDesc &d = inst_at(e, ic, i);
+                const PackedField<R> f = packed_of<R>(d);
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    store_link<R>(f, cur.ps.s, 2 * role + j, up[j]);
+                    store_link<R>(f, cur.ps.sd[j], 2 * role + j, dn[j]);
+                }
+                if (SITE_W) {
+#pragma unroll
+                    for (int r = 0; r < 3; r++)
+                        d.w[(int64_t)(role * 3 + r) * d.g.V + cur.ps.s] =
+                            make_float2((float)wcol[r].x, (float)wcol[r].y);
+                }
+            }
+        }
+        cur = nxt;
     }
 }
 
@@ -720,7 +910,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_batched_pass_staged(EngineDev e,
             unstage_link<R>(wbase + cur * NCH * 32, Chunks<R>::per_link, dn);
             Rng<R> rng;
             if (ALGO == ALG_SA || ALGO == ALG_SR || ALGO == ALG_RANDOM)
-                rng.init(ref_rng_tid(t.h), p.seed + (uint32_t)t.inst, p.counter);
+                rng.init(ref_rng_tid(t.h), inst_seed(p, t.inst), inst_counter(p, t.inst));
             site_update<GAUGE, ALGO>(up, dn, mu, p, rng);
             const PackedField<R> f = packed_of<R>(d);
             store_link<R>(f, t.s, mu, up);
@@ -849,7 +1039,7 @@ __global__ void __launch_bounds__(128, 2) k_batched_pass_site_staged(EngineDev e
             }
             Rng<float> rng;
             if (ALGO == ALG_SA || ALGO == ALG_SR || ALGO == ALG_RANDOM)
-                rng.init(ref_rng_tid(h), p.seed + (uint32_t)inst, p.counter);
+                rng.init(ref_rng_tid(h), inst_seed(p, inst), inst_counter(p, inst));
             site_update_thread<GAUGE, ALGO, float, SITE_W>(up, dn, p, rng, &wc);
             const PackedField<float> f = packed_of<float>(d);
 #pragma unroll

@@ -113,6 +113,7 @@ static int plugin_step(int gauge, int real, int algo, void *U, void *Udw, const 
     a.p.param = param;
     a.p.seed = (uint32_t)seed;
     a.p.counter = (uint32_t)counter;
+    a.p.counter_stride = 0;
     a.stream = (cudaStream_t)stream;
     return dispatch_gauge_algo<RefStep>(gauge, algo, a);
 }

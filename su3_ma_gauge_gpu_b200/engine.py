@@ -55,6 +55,7 @@ class Schedule:
     fold: int = 1          # refine contexts: iterative refinement below switch_theta (0: FP64 sweeps)
     trace_checks: int = 0  # > 0: keep that many OR checks per instance for GaugeFixer.trace()
     fold_exit: float = 4.0  # fold mode: FP64 sweeps once the master's theta < fold_exit * precision
+    rng_streams: int = 0    # 1: one Philox stream through the instances, as the apps draw it (no SR)
 
     @classmethod
     def mag_app(cls, **kw) -> "Schedule":

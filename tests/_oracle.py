@@ -111,6 +111,51 @@ def fix(U, size, gauge, sched: Schedule, counter=0, nthreads=8):
     return r, c.value
 
 
+class AppSchedule(ctypes.Structure):
+    """orc_app_schedule of oracle/gf_oracle.h: the apps' per-copy loop for every gauge."""
+
+    _fields_ = [("random_trafo", ctypes.c_int), ("sa_steps", ctypes.c_int), ("sa_min", ctypes.c_float),
+                ("sa_max", ctypes.c_float), ("micro_updates", ctypes.c_int), ("sa_mode", ctypes.c_int),
+                ("sa_repeat", ctypes.c_int), ("sa_slow_lo", ctypes.c_double), ("sa_slow_hi", ctypes.c_double),
+                ("sa_slow_factor", ctypes.c_float), ("sr_max_iter", ctypes.c_int), ("sr_parameter", ctypes.c_float),
+                ("sr_stop_theta", ctypes.c_double), ("or_max_iter", ctypes.c_int), ("or_parameter", ctypes.c_float),
+                ("precision", ctypes.c_float), ("check_precision", ctypes.c_int), ("reproject", ctypes.c_int),
+                ("seed", ctypes.c_uint32)]
+
+
+class AppResult(ctypes.Structure):
+    _fields_ = [("gff", ctypes.c_double), ("theta", ctypes.c_double), ("or_iterations", ctypes.c_int),
+                ("sa_sweeps", ctypes.c_int), ("sr_iterations", ctypes.c_int)]
+
+
+def app_schedule(**kw) -> AppSchedule:
+    """An AppSchedule with the apps' defaults (apps/program_options/ProgramOptions.hxx:223-266)."""
+    base = dict(random_trafo=0, sa_steps=0, sa_min=0.01, sa_max=0.4, micro_updates=0, sa_mode=0, sa_repeat=1,
+                sa_slow_lo=0.0, sa_slow_hi=0.0, sa_slow_factor=1.0, sr_max_iter=0, sr_parameter=1.7,
+                sr_stop_theta=1e-6, or_max_iter=1000, or_parameter=1.7, precision=1e-7, check_precision=100,
+                reproject=100, seed=1)
+    base.update(kw)
+    return AppSchedule(**base)
+
+
+def fix_app(U, size, gauge, sched: AppSchedule, counter=0, Udw=None, nthreads=8):
+    """orc_fix_app in place on U (and Udw for Coulomb); returns (AppResult, counter after)."""
+    c = _u32(counter)
+    r = AppResult()
+    getattr(oracle(), "orc_fix_app_" + sfx(U))(_ptr(U), _ptr(Udw), _ptr(_size(size)), gauge, ctypes.byref(sched),
+                                               ctypes.byref(c), ctypes.byref(r), nthreads)
+    return r, c.value
+
+
+def fix_coulomb(U, size, sched: AppSchedule, counter=0, nthreads=8):
+    """orc_fix_coulomb in place on the GpuPatternTimeslice array U; returns ([AppResult] per slice, counter)."""
+    c = _u32(counter)
+    res = (AppResult * int(size[0]))()
+    getattr(oracle(), "orc_fix_coulomb_" + sfx(U))(_ptr(U), _ptr(_size(size)), ctypes.byref(sched), ctypes.byref(c),
+                                                   res, nthreads)
+    return list(res), c.value
+
+
 # ---- the reference's own code on the host (oracle/_ref) ----------------------------------------
 def ref_step(U, size, gauge, algo, parity, param=0.0, seed=0, counter=0, Udw=None):
     lib = ref_pin(sfx(U))

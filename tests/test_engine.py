@@ -165,6 +165,91 @@ def test_fix_reprojection_cadence_matches_oracle_driver(cuda, reproject, check):
             assert np.abs(out - ref).max() < 1e-9
 
 
+def test_landau_app_fix_with_sa_matches_oracle_driver(cuda):
+    """The Landau app's whole loop in FP64 -- random gauge transformation, SA with linearly falling
+    temperature and microcanonical steps after every SA sweep, OR to theta < 1e-12, reprojections --
+    through gf_fix and through the oracle's restatement (apps/LandauGaugeFixingSU3_4D.cu:185-271) on
+    the same input and Philox key/counters: the same sweep counts, functional and field."""
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer, Schedule
+
+    size = (4, 4, 4, 8)
+    U, _ = S.smooth_config(size, 0.3, 93)
+    prec = float(np.float32(1e-12))
+    kw = dict(random_trafo=1, sa_steps=12, sa_min=0.01, sa_max=0.8, micro_updates=2, or_max_iter=4000,
+              precision=prec, check_precision=10, reproject=7, seed=21)
+    with GaugeFixer([size], mixed=False) as gf:
+        gf.load(0, U)
+        rep = gf.fix(Schedule(rng_counter=6, **kw))[0]
+        out = np.zeros_like(U)
+        gf.store(0, out)
+    ref = U.copy()
+    r, ctr = O.fix_app(ref, size, O.LANDAU, O.app_schedule(**kw), counter=6)
+    assert ctr == 6 + 2 + 2 * 12
+    assert (rep.sa_sweeps, rep.or_sweeps) == (r.sa_sweeps, r.or_iterations)
+    assert rep.converged and r.theta < 1e-12
+    assert rep.gff == pytest.approx(r.gff, rel=1e-10)
+    assert np.abs(out - ref).max() < 1e-9
+
+
+def test_mag_app_fix_matches_oracle_driver(cuda):
+    """The MAG app's whole schedule in FP64 -- random trafo, the SA do-while (5 heat-bath sweeps, each
+    with a microcanonical sweep, per temperature, the step slowed 15x in [0.7, 0.88]), SR until
+    theta < 1e-6, OR to theta < 1e-12, reprojections -- through gf_fix and through the oracle's
+    restatement of apps/MAGaugeFixingSU3_4D.cu:222-333 on the same input and Philox key/counters:
+    the same sweep count in every phase, the same functional and field."""
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer, Schedule
+
+    size = (4, 4, 4, 8)
+    U, _ = S.smooth_config(size, 0.3, 91)
+    prec = float(np.float32(1e-12))
+    sch = Schedule.mag_app(random_trafo=1, sa_steps=8, sa_min=0.01, sa_max=1.4, micro_updates=1, or_max_iter=4000,
+                           precision=prec, check_precision=10, reproject=20, seed=3, rng_counter=5)
+    with GaugeFixer([size], gauge="mag", mixed=False) as gf:
+        gf.load(0, U)
+        rep = gf.fix(sch)[0]
+        out = np.zeros_like(U)
+        gf.store(0, out)
+    ref = U.copy()
+    osch = O.app_schedule(random_trafo=1, sa_steps=8, sa_min=0.01, sa_max=1.4, micro_updates=1, sa_mode=2,
+                          sa_repeat=5, sa_slow_lo=0.7, sa_slow_hi=0.88, sa_slow_factor=15.0, sr_max_iter=1000,
+                          sr_parameter=1.7, sr_stop_theta=1e-6, or_max_iter=4000, precision=prec, check_precision=10,
+                          reproject=20, seed=3)
+    r, _ = O.fix_app(ref, size, O.MAG, osch, counter=5)
+    assert (rep.sa_sweeps, rep.sr_sweeps, rep.or_sweeps) == (r.sa_sweeps, r.sr_iterations, r.or_iterations)
+    assert rep.converged and r.theta < 1e-12
+    assert rep.gff == pytest.approx(r.gff, rel=1e-10)
+    assert np.abs(out - ref).max() < 1e-9
+
+
+def test_coulomb_app_fix_matches_oracle_slice_loop(cuda):
+    """The Coulomb app's loop (apps/CoulombGaugeFixingSU3_4D.cu:199-311): timeslices one after the
+    other, each with random trafo, SA + a microcanonical sweep after every SA sweep, OR to
+    theta < 1e-12, the Philox counter running on from slice to slice.  gf_fix batches all slices and,
+    with rng_streams = 1, gives each slice the key word and counters the app's loop gives it: per
+    slice the same sweep counts and functional, and the same exported field -- temporal links
+    included, which the app multiplies from both sides one slice at a time."""
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer, Schedule
+
+    size = (4, 4, 6, 4)
+    U = np.concatenate([S.smooth_config((1,) + size[1:], 0.3, 140 + t)[0] for t in range(size[0])])
+    prec = float(np.float32(1e-12))
+    kw = dict(random_trafo=1, sa_steps=5, sa_min=0.01, sa_max=1.0, micro_updates=1, or_max_iter=4000, precision=prec,
+              check_precision=10, reproject=20, seed=11)
+    with GaugeFixer([size], gauge="coulomb", mixed=False) as gf:
+        gf.load(0, U)
+        reps = gf.fix(Schedule(rng_counter=4, rng_streams=1, **kw))
+        out = np.zeros_like(U)
+        gf.store(0, out)
+    ref = U.copy()
+    res, ctr = O.fix_coulomb(ref, size, O.app_schedule(**kw), counter=4)
+    assert ctr == 4 + size[0] * 12
+    for t in range(size[0]):
+        assert (reps[t].sa_sweeps, reps[t].or_sweeps) == (res[t].sa_sweeps, res[t].or_iterations), t
+        assert reps[t].converged and res[t].theta < 1e-12
+        assert reps[t].gff == pytest.approx(res[t].gff, rel=1e-10), t
+    assert np.abs(out - ref).max() < 1e-9
+
+
 def _mixed_vs_fp64(size, eps, seed):
     from su3_ma_gauge_gpu_b200.engine import GaugeFixer
 
@@ -200,18 +285,21 @@ def test_fix_mixed_rough_field_reports_copy(cuda):
 @pytest.mark.parametrize("prec", ["fp32", "fp64", "refine"])
 def test_pipelined_pass_bit_identical_to_direct(cuda, prec):
     """Every launch shape of the OR pass -- cp.async-pipelined (2, 4, 8 warps per block), register
-    prefetch (persistent), 64-register FP32 -- computes exactly what the direct pass computes, on a
-    batch of uneven lattices; in refine mode including the accumulated W (the export applies it)."""
+    prefetch (persistent), 64-register FP32, thread per site, two lanes per site (direct and
+    persistent) -- computes exactly what the direct pass computes, on a batch of uneven lattices
+    (the first has 3 eight-site tiles, so two-lane warps straddle instances); in refine mode
+    including the accumulated W (the export applies it)."""
     from su3_ma_gauge_gpu_b200.engine import GaugeFixer
 
-    sizes = [(4, 4, 4, 4), (2, 6, 4, 8), (8, 8, 8, 8)]
+    sizes = [(2, 2, 2, 6), (4, 4, 4, 4), (2, 6, 4, 8), (8, 8, 8, 8)]
     fields = [S.smooth_config(s, 0.3, 50 + i)[0] for i, s in enumerate(sizes)]
     mixed = {"fp32": True, "fp64": False, "refine": "refine"}[prec]
     outs = {}
     if prec == "refine":
-        shapes = [(0, 4), (2, 4), (3, 4), (4, 4), (5, 4)]
+        shapes = [(0, 4), (2, 4), (3, 4), (4, 4), (5, 4), (6, 4), (7, 4)]
     else:
-        shapes = [(0, 4), (1, 2), (1, 4), (1, 8), (3, 4)] + ([(2, 4), (4, 4), (5, 4)] if prec == "fp32" else [])
+        shapes = [(0, 4), (1, 2), (1, 4), (1, 8), (3, 4), (6, 4)] + ([(2, 4), (4, 4), (5, 4), (7, 4)]
+                                                                     if prec == "fp32" else [])
     for variant, warps in shapes:
         with GaugeFixer(sizes, mixed=mixed) as gf:
             gf.set_pass_shape("fp64" if prec == "fp64" else "fp32", variant, warps)
@@ -261,6 +349,37 @@ def test_thread_per_site_pass_matches_direct(cuda, gauge, algo):
         assert np.abs(a - b).max() < tol
 
 
+@pytest.mark.parametrize("prec", ["fp32", "fp64", "refine"])
+@pytest.mark.parametrize("gauge", ["landau", "mag", "u1xu1"])
+@pytest.mark.parametrize("algo", ["sa", "micro", "sr", "random"])
+def test_two_lane_pass_matches_direct(cuda, gauge, algo, prec):
+    """The two-lanes-per-site pass sums the four directions in the 4-lane butterfly's order and both
+    lanes of a site draw the Philox numbers the direct pass draws, for every update rule: one sweep
+    agrees with the direct pass to FP32 rounding (FP64: 1e-13)."""
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer
+
+    sizes = [(2, 2, 2, 6), (4, 4, 4, 4), (2, 6, 4, 8)]
+    fields = [S.smooth_config(s, 0.3, 75 + i)[0] for i, s in enumerate(sizes)]
+    mixed = {"fp32": True, "fp64": False, "refine": "refine"}[prec]
+    real = "fp64" if prec == "fp64" else "fp32"
+    outs = []
+    for variant in (0, 6):
+        with GaugeFixer(sizes, gauge=gauge, mixed=mixed) as gf:
+            gf.set_pass_shape(real, variant, 4)
+            for i, U in enumerate(fields):
+                gf.load(i, U)
+            gf.sweeps(algo, 1, 0.7, 5, 11)
+            res = []
+            for i, U in enumerate(fields):
+                o = np.zeros_like(U)
+                gf.store(i, o)
+                res.append(o)
+            outs.append(res)
+    tol = 1e-13 if prec == "fp64" else (1e-4 if (gauge, algo) == ("u1xu1", "micro") else 1e-5)
+    for a, b in zip(*outs):
+        assert np.abs(a - b).max() < tol
+
+
 def test_autotune_picks_a_shape(cuda):
     from su3_ma_gauge_gpu_b200.engine import GaugeFixer
 
@@ -271,7 +390,7 @@ def test_autotune_picks_a_shape(cuda):
         before = np.zeros_like(U)
         gf.store(0, before)
         c32, c64 = gf.autotune()
-        assert c32 in (0, 64, 100, 32, 33, 2, 4, 8) and c64 in (0, 100, 2, 4, 8)
+        assert c32 in (0, 64, 100, 32, 33, 16, 116, 2, 4, 8) and c64 in (0, 100, 16, 2, 4, 8)
         after = np.zeros_like(U)
         gf.store(0, after)
         assert np.array_equal(before, after)  # tuning ran on a scratch copy
