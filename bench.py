@@ -403,7 +403,9 @@ def run_gribov(args, steps=None, warmup=None):
 
 def run_plain8(args, steps=None, warmup=None):
     """The 8^4 plain-method configuration: Haar-random links, FP64 (the reference's full 18-real
-    array in, out), OR omega = 1.7 to theta < 1e-12, at most 20000 sweeps; timed per fix."""
+    array in, out), OR omega = 1.7 to theta < 1e-12, at most 20000 sweeps; timed per fix, once with
+    one launch per parity pass (check chunks replayed from CUDA graphs) and once with one persistent
+    cooperative launch per check chunk."""
     import numpy as np
     import torch
 
@@ -413,33 +415,37 @@ def run_plain8(args, steps=None, warmup=None):
     steps = args.steps if steps is None else steps
     warmup = args.warmup if warmup is None else warmup
     size = (8, 8, 8, 8)
+    V = int(np.prod(size))
     U = torch.from_numpy(S.hot_config(size, 4242)).cuda()
     out = torch.empty_like(U)
     stream = torch.cuda.Stream()
-    sched = Schedule(or_max_iter=20000, precision=1e-12, check_precision=args.check, reproject=100,
-                     micro_updates=0)
-    with GaugeFixer([size], mixed=False, stream=stream) as gf:
-        gf.load(0, U)
-        gf.autotune()
-        rep = None
-        for _ in range(warmup):
+    res = {"workload": "plain8", "steps": steps, "warmup": warmup}
+    for name, persistent in (("per_pass_launches", 0), ("persistent_chunks", 1)):
+        sched = Schedule(or_max_iter=20000, precision=1e-12, check_precision=args.check, reproject=100,
+                         micro_updates=0, persistent=persistent)
+        with GaugeFixer([size], mixed=False, stream=stream) as gf:
             gf.load(0, U)
-            rep = gf.fix(sched)[0]
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(max(1, steps)):
-            gf.load(0, U)
-            rep = gf.fix(sched)[0]
-            gf.store(0, out)
-        e1.record(stream)
-        torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / max(1, steps)
-    V = int(np.prod(size))
-    return {"workload": "plain8", "steps": steps, "warmup": warmup, "ms_per_fix": ms, "or_sweeps": rep.or_sweeps,
-            "theta": rep.theta, "F": rep.gff, "converged": rep.converged,
-            "us_per_sweep": ms * 1e3 / max(1, rep.or_sweeps),
-            "gsite_updates_per_s": V * rep.or_sweeps / (ms * 1e-3) / 1e9}
+            gf.autotune()
+            rep = None
+            for _ in range(warmup):
+                gf.load(0, U)
+                rep = gf.fix(sched)[0]
+            torch.cuda.synchronize()
+            l0 = gf.kernel_launches()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(max(1, steps)):
+                gf.load(0, U)
+                rep = gf.fix(sched)[0]
+                gf.store(0, out)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            launches = (gf.kernel_launches() - l0) / max(1, steps)
+        ms = e0.elapsed_time(e1) / max(1, steps)
+        res[name] = {"ms_per_fix": ms, "or_sweeps": rep.or_sweeps, "theta": rep.theta, "F": rep.gff,
+                     "converged": rep.converged, "us_per_sweep": ms * 1e3 / max(1, rep.or_sweeps),
+                     "gsite_updates_per_s": V * rep.or_sweeps / (ms * 1e-3) / 1e9, "kernel_launches": launches}
+    return res
 
 
 def run_coulomb48(args, steps=None, warmup=None):

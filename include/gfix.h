@@ -206,6 +206,17 @@ typedef struct gf_schedule {
                               trafo and SA; not with sr_max_iter > 0) -- for a Coulomb lattice the
                               timeslices then draw exactly what apps/CoulombGaugeFixingSU3_4D.cu
                               draws for them */
+    int persistent;        /* 1: each check chunk's OR sweeps (and its reprojections) run as ONE
+                              cooperative launch per precision, the parity passes separated by a
+                              grid-wide barrier, instead of one launch per pass (the apps' loop,
+                              apps/LandauGaugeFixingSU3_4D.cu:244-262, launches two kernels per
+                              sweep); for small lattices, whose passes are shorter than a launch.
+                              Contexts without the separate W array only (plain FP64, mixed = 1,
+                              GF_COULOMB), check_precision <= 256; else GF_ERR_UNSUPPORTED */
+    int wait_budget_us;    /* persistent: bound of every barrier wait (0: 1 s); a wait that runs out
+                              stops the kernel and gf_fix returns GF_ERR_TIMEOUT, the context usable */
+    int wait_test_missing; /* persistent: barrier arrivals that never come -- only for testing the
+                              bounded wait; 0 in use */
 } gf_schedule;
 
 typedef struct gf_report {

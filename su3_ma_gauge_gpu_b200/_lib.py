@@ -77,7 +77,8 @@ class Schedule(ctypes.Structure):
                 ("sa_slow_factor", ctypes.c_float), ("sr_max_iter", ctypes.c_int), ("sr_parameter", ctypes.c_float),
                 ("sr_stop_theta", ctypes.c_double), ("stall_checks", ctypes.c_int),
                 ("fold", ctypes.c_int), ("trace_checks", ctypes.c_int), ("fold_exit", ctypes.c_double),
-                ("rng_streams", ctypes.c_int)]
+                ("rng_streams", ctypes.c_int), ("persistent", ctypes.c_int), ("wait_budget_us", ctypes.c_int),
+                ("wait_test_missing", ctypes.c_int)]
 
 
 class Report(ctypes.Structure):

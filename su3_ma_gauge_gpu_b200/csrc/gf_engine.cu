@@ -21,6 +21,34 @@
 
 using namespace gfb;
 
+namespace {
+
+bool same_check(const CheckParams &a, const CheckParams &b)
+{
+    return a.want_state == b.want_state && a.chunk_sweeps == b.chunk_sweeps && a.max_sweeps == b.max_sweeps &&
+           a.switch_theta == b.switch_theta && a.precision == b.precision && a.stop_max == b.stop_max &&
+           a.transitions == b.transitions && a.stall_checks == b.stall_checks && a.fold == b.fold &&
+           a.fold_exit == b.fold_exit;
+}
+
+// what a captured check chunk depends on besides the context's buffers and launch shapes
+struct ChunkKey {
+    int n = 0, has32 = 0, has64 = 0, persistent = 0;
+    unsigned int missing = 0;
+    unsigned long long budget_ns = 0;
+    float omega = 0.f;
+    std::vector<unsigned char> repro;
+    CheckParams base{};
+    bool operator==(const ChunkKey &o) const
+    {
+        return n == o.n && has32 == o.has32 && has64 == o.has64 && persistent == o.persistent &&
+               missing == o.missing && budget_ns == o.budget_ns && omega == o.omega && repro == o.repro &&
+               same_check(base, o.base);
+    }
+};
+
+}  // namespace
+
 struct gf_ctx {
     int gauge = 0, ninst = 0, mixed = 0, device = 0;
     int refine = 0;           // mixed mode 2: FP64 master + FP32 working copy + accumulated W
@@ -51,6 +79,23 @@ struct gf_ctx {
     mutable long long launches = 0;  // kernels this context has launched (graph nodes per replay)
     int num_sms = 148;
     uint32_t counter_stride = 0;  // Philox streams of the batch (AlgoParams::counter_stride), set by gf_fix
+    // persistent chunk kernel: grid-barrier state on the device, and the {error, barrier} words of the
+    // last two chunks in pinned memory
+    ChunkSync *d_sync = nullptr;
+    unsigned int *h_sync = nullptr;
+    // check chunks captured as graphs, kept for later gf_fix calls; dropped when the launch shapes or
+    // the trace buffer change (the graphs hold both)
+    struct Graph {
+        ChunkKey key;
+        cudaGraphExec_t exec;
+        long long nodes;
+    };
+    std::vector<Graph> graphs;
+    void drop_graphs()
+    {
+        for (auto &g : graphs) cudaGraphExecDestroy(g.exec);
+        graphs.clear();
+    }
     // parity-pass launch shape per precision ([0] FP32, [1] FP64): variant 0 = one warp per
     // 8-site tile, 128 threads per block; variant 1 = pipelined (cp.async prefetch of the next
     // tile), `warps` warps per block, grid = num_sms * blocks_per_sm
@@ -374,16 +419,77 @@ int check_ctx(gf_ctx *c)
 // right after sweep i when i % reproject == 0, apps/LandauGaugeFixingSU3_4D.cu:249-252), then the
 // checks: FP64 first, then FP32 with the switch of the instances that crossed switch_theta (so a
 // switched instance is not counted twice).
+struct ChunkOpts {
+    int persistent;                 // 1: one cooperative launch per precision for the chunk's sweeps
+    unsigned long long budget_ns;   // bound of every grid-barrier wait
+    unsigned int missing;           // barrier arrivals that never come (tests of the bounded wait)
+};
+
+template <typename R, int GAUGE>
+int launch_chunk_g(gf_ctx *c, int want, int nsweeps, const ChunkReproject &rp, float omega, const ChunkOpts &po)
+{
+    auto kern = k_chunk_sweeps<R, GAUGE>;
+    static int occ_cached = 0;  // co-resident blocks per SM: a cooperative grid may not exceed them
+    if (occ_cached <= 0) {
+        int o = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, 128, 0) != cudaSuccess || o < 1) o = 1;
+        occ_cached = o;
+    }
+    const int64_t need = (c->total_warps + 3) / 4;
+    const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)c->num_sms * occ_cached));
+    int st = cuda_status(cudaMemsetAsync(c->d_sync, 0, sizeof(ChunkSync), c->stream), "barrier reset");
+    if (st) return st;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(128);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = c->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    const AlgoParams p{omega, 0u, 0u, 0u};
+    st = cuda_status(cudaLaunchKernelEx(&cfg, kern, c->dev(), c->total_warps, c->total_links, nsweeps, rp, p, want,
+                                        c->d_sync, blocks + po.missing, po.budget_ns),
+                     "persistent chunk launch");
+    c->launches++;
+    return st;
+}
+
+int launch_chunk(gf_ctx *c, int want, int nsweeps, const ChunkReproject &rp, float omega, const ChunkOpts &po)
+{
+    const bool f32 = want == ST_FP32;
+    switch (c->gauge) {
+    case LANDAU: return f32 ? launch_chunk_g<float, LANDAU>(c, want, nsweeps, rp, omega, po)
+                            : launch_chunk_g<double, LANDAU>(c, want, nsweeps, rp, omega, po);
+    case COULOMB: return f32 ? launch_chunk_g<float, COULOMB>(c, want, nsweeps, rp, omega, po)
+                             : launch_chunk_g<double, COULOMB>(c, want, nsweeps, rp, omega, po);
+    case MAG: return f32 ? launch_chunk_g<float, MAG>(c, want, nsweeps, rp, omega, po)
+                         : launch_chunk_g<double, MAG>(c, want, nsweeps, rp, omega, po);
+    default: return f32 ? launch_chunk_g<float, U1XU1>(c, want, nsweeps, rp, omega, po)
+                        : launch_chunk_g<double, U1XU1>(c, want, nsweeps, rp, omega, po);
+    }
+}
+
 int enqueue_or_chunk(gf_ctx *c, int nsweeps, float omega, const std::vector<unsigned char> &reproject_after,
-                     const CheckParams &base, bool has32, bool has64)
+                     const CheckParams &base, bool has32, bool has64, const ChunkOpts &po)
 {
     int st = GF_OK;
-    for (int k = 0; k < nsweeps && !st; k++) {
-        if (has32) st = launch_sweep(c, ALG_OR, ST_FP32, omega, 0, 0, 0);
-        if (!st && has64) st = launch_sweep(c, ALG_OR, ST_FP64, omega, 0, 0, 0);
-        if (!st && reproject_after[k]) {
-            if (has32) st = launch_reunitarise(c, ST_FP32, false);
-            if (!st && has64) st = launch_reunitarise(c, ST_FP64, false);
+    if (po.persistent) {
+        ChunkReproject rp{};
+        for (int k = 0; k < nsweeps; k++)
+            if (reproject_after[k]) rp.bits[k >> 6] |= 1ull << (k & 63);
+        if (has32) st = launch_chunk(c, ST_FP32, nsweeps, rp, omega, po);
+        if (!st && has64) st = launch_chunk(c, ST_FP64, nsweeps, rp, omega, po);
+    } else {
+        for (int k = 0; k < nsweeps && !st; k++) {
+            if (has32) st = launch_sweep(c, ALG_OR, ST_FP32, omega, 0, 0, 0);
+            if (!st && has64) st = launch_sweep(c, ALG_OR, ST_FP64, omega, 0, 0, 0);
+            if (!st && reproject_after[k]) {
+                if (has32) st = launch_reunitarise(c, ST_FP32, false);
+                if (!st && has64) st = launch_reunitarise(c, ST_FP64, false);
+            }
         }
     }
     if (st) return st;
@@ -577,6 +683,9 @@ int gf_destroy(gf_ctx *c)
 {
     if (!c) return GF_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
+    c->drop_graphs();
+    cudaFree(c->d_sync);
+    if (c->h_sync) cudaFreeHost(c->h_sync);
     cudaFree(c->f32);
     cudaFree(c->f64);
     cudaFree(c->t64);
@@ -836,6 +945,19 @@ int gf_set_storage(gf_ctx *c, int real)
     return GF_OK;  // FP32 request on a mixed context: instances start in FP32 at import
 }
 
+namespace {
+
+// the {error, barrier} words a persistent chunk left in slot `slot`
+int chunk_timeout(gf_ctx *c, int slot, const ChunkOpts &po)
+{
+    if (!c->h_sync[2 * slot]) return GF_OK;
+    set_error("persistent chunk kernel: a grid-barrier wait ran out of its %llu ns budget at barrier %u",
+              (unsigned long long)po.budget_ns, c->h_sync[2 * slot + 1]);
+    return GF_ERR_TIMEOUT;
+}
+
+}  // namespace
+
 int gf_fix(gf_ctx *c, const gf_schedule *s, gf_report *rep)
 {
     clear_error();
@@ -962,6 +1084,7 @@ int gf_fix(gf_ctx *c, const gf_schedule *s, gf_report *rep)
     }
     // optional check trace: (re)allocated for this run's capacity, or switched off
     if (s->trace_checks > 0 && s->trace_checks != c->trace_cap) {
+        c->drop_graphs();
         cudaFree(c->d_trace);
         cudaFree(c->d_ntrace);
         c->d_trace = nullptr;
@@ -973,6 +1096,7 @@ int gf_fix(gf_ctx *c, const gf_schedule *s, gf_report *rep)
             return st;
         c->trace_cap = s->trace_checks;
     } else if (s->trace_checks <= 0 && c->trace_cap) {
+        c->drop_graphs();
         cudaFree(c->d_trace);
         cudaFree(c->d_ntrace);
         c->d_trace = nullptr;
@@ -984,18 +1108,38 @@ int gf_fix(gf_ctx *c, const gf_schedule *s, gf_report *rep)
         return st;
     if ((st = sync_states(c))) return st;
     const int C = s->check_precision;
-    struct Variant {
-        int n;
-        std::vector<unsigned char> repro;
-        int has32, has64;
-        cudaGraphExec_t exec;
-        long long nodes;
-    };
-    std::vector<Variant> graphs;
+    // one persistent launch per check chunk (schedule.persistent): not for contexts with the separate
+    // W array, and at most 256 sweeps per chunk (the reprojection mask)
+    ChunkOpts po{s->persistent ? 1 : 0, 1000000000ull, 0u};
+    if (po.persistent) {
+        if (c->site_w || C > 256 || s->wait_test_missing < 0) {
+            set_error("persistent chunks need a context without the separate W array (plain FP64, FP32 storage or "
+                      "Coulomb) and check_precision <= 256");
+            return GF_ERR_UNSUPPORTED;
+        }
+        if (s->wait_budget_us > 0) po.budget_ns = 1000ull * (unsigned long long)s->wait_budget_us;
+        po.missing = (unsigned int)s->wait_test_missing;
+        if (!c->d_sync && (st = cuda_status(cudaMalloc(&c->d_sync, sizeof(ChunkSync)), "cudaMalloc barrier")))
+            return st;
+        if (!c->h_sync && (st = cuda_status(cudaHostAlloc(&c->h_sync, sizeof(unsigned int) * 4, cudaHostAllocDefault),
+                                            "cudaHostAlloc")))
+            return st;
+        c->h_sync[0] = c->h_sync[2] = 0;
+    }
     auto get_graph = [&](int n, const std::vector<unsigned char> &repro, int h32, int h64,
                          cudaGraphExec_t &out) -> int {
-        for (auto &v : graphs)
-            if (v.n == n && v.repro == repro && v.has32 == h32 && v.has64 == h64) {
+        ChunkKey key;
+        key.n = n;
+        key.has32 = h32;
+        key.has64 = h64;
+        key.persistent = po.persistent;
+        key.missing = po.missing;
+        key.budget_ns = po.budget_ns;
+        key.omega = s->or_parameter;
+        key.repro = repro;
+        key.base = base;
+        for (auto &v : c->graphs)
+            if (v.key == key) {
                 out = v.exec;
                 c->launches += v.nodes;
                 return GF_OK;
@@ -1004,7 +1148,7 @@ int gf_fix(gf_ctx *c, const gf_schedule *s, gf_report *rep)
         int r = cuda_status(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
         if (r) return r;
         const long long before = c->launches;
-        r = enqueue_or_chunk(c, n, s->or_parameter, repro, base, h32, h64);
+        r = enqueue_or_chunk(c, n, s->or_parameter, repro, base, h32, h64, po);
         const long long nodes = c->launches - before;
         const int r2 = cuda_status(cudaStreamEndCapture(c->stream, &g), "end capture");
         if (r || r2) {
@@ -1015,7 +1159,7 @@ int gf_fix(gf_ctx *c, const gf_schedule *s, gf_report *rep)
         r = cuda_status(cudaGraphInstantiate(&ex, g, 0), "graph instantiate");
         cudaGraphDestroy(g);
         if (r) return r;
-        graphs.push_back(Variant{n, repro, h32, h64, ex, nodes});
+        c->graphs.push_back(gf_ctx::Graph{key, ex, nodes});
         out = ex;
         return GF_OK;
     };
@@ -1039,10 +1183,14 @@ int gf_fix(gf_ctx *c, const gf_schedule *s, gf_report *rep)
             cudaGraphExec_t ex = nullptr;
             if ((st = get_graph(n, repro, has32, has64, ex))) break;
             if ((st = cuda_status(cudaGraphLaunch(ex, c->stream), "graph launch"))) break;
-        } else if ((st = enqueue_or_chunk(c, n, s->or_parameter, repro, base, has32, has64))) {
+        } else if ((st = enqueue_or_chunk(c, n, s->or_parameter, repro, base, has32, has64, po))) {
             break;
         }
         issued += n;
+        if (po.persistent && (st = cuda_status(cudaMemcpyAsync(c->h_sync + 2 * (k & 1), &c->d_sync->error,
+                                                               2 * sizeof(unsigned int), cudaMemcpyDeviceToHost,
+                                                               c->stream), "barrier status copy")))
+            break;
         if ((st = cuda_status(cudaMemcpyAsync(c->h_chunk + (k & 1) * 2 * c->ninst, c->d_state,
                                               sizeof(int) * 2 * c->ninst, cudaMemcpyDeviceToHost, c->stream),
                               "state copy")))
@@ -1053,6 +1201,7 @@ int gf_fix(gf_ctx *c, const gf_schedule *s, gf_report *rep)
             // slot (k-1) & 1 holds the complete copy of chunk k-1 once its event has fired; chunk k's
             // copy lands in the other slot and is read in the next iteration
             if ((st = cuda_status(cudaEventSynchronize(c->ev_chunk[(k - 1) & 1]), "event sync"))) break;
+            if (po.persistent && (st = chunk_timeout(c, (k - 1) & 1, po))) break;
             bool a2, h32b, h64b;
             scan(c->h_chunk + ((k - 1) & 1) * 2 * c->ninst, a2, h32b, h64b);
             any_active = a2;
@@ -1062,9 +1211,12 @@ int gf_fix(gf_ctx *c, const gf_schedule *s, gf_report *rep)
             has64 = h64b;
         }
     }
-    for (auto &v : graphs) cudaGraphExecDestroy(v.exec);
-    if (st) return st;
+    if (st) {
+        cudaStreamSynchronize(c->stream);
+        return st;
+    }
     if ((st = cuda_status(cudaStreamSynchronize(c->stream), "sync"))) return st;
+    if (po.persistent && launched > 0 && (st = chunk_timeout(c, (launched - 1) & 1, po))) return st;
     if (rep) {
         if ((st = cuda_status(cudaMemcpy(c->h_quality, c->d_quality, sizeof(double) * 2 * c->ninst,
                                          cudaMemcpyDeviceToHost), "quality copy")))
@@ -1190,6 +1342,7 @@ int gf_autotune(gf_ctx *c, int *choice_fp32, int *choice_fp64)
         if (st) return st;
         c->shape[prec] = cands[besti];
         c->tuned[prec] = 1;
+        c->drop_graphs();
     }
     auto code = [](const gf_ctx::PassShape &sh) {
         return sh.variant == 1 ? sh.warps
@@ -1221,6 +1374,7 @@ int gf_set_pass_shape(gf_ctx *c, int real, int variant, int warps)
                   "pipelined; the 64-register and thread-per-site passes are FP32)");
         return GF_ERR_INVALID;
     }
+    c->drop_graphs();
     c->shape[real].variant = variant;
     c->shape[real].warps = warps;
     c->shape[real].blocks_per_sm = 0;

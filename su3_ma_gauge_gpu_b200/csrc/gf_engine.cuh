@@ -1061,6 +1061,137 @@ __global__ void __launch_bounds__(128, 2) k_batched_pass_site_staged(EngineDev e
     cp_async_wait<0>();
 }
 
+// ---- one persistent launch per check chunk --------------------------------------------------------
+// A cooperative launch (every block resident) runs all parity passes of a check chunk -- and the
+// reprojections the drivers do inside it -- with a grid-wide barrier between them, instead of one
+// launch per pass: for small lattices the launches, not the passes, set the time per sweep.
+// Every wait of the barrier is bounded: a block that waits longer than budget_ns records the
+// barrier in ChunkSync and leaves the kernel, and every other block leaves at its next wait, so the
+// host gets an error status (GF_ERR_TIMEOUT) and the context stays usable.
+struct ChunkSync {
+    unsigned int count;   // blocks arrived at the current barrier
+    unsigned int gen;     // barrier generation
+    unsigned int error;   // 1: a wait ran out of its budget
+    unsigned int where;   // index of that barrier
+};
+
+struct ChunkReproject {
+    unsigned long long bits[4];  // bit k: reproject after sweep k of the chunk (k < 256)
+    __device__ __forceinline__ bool after(int k) const { return (bits[k >> 6] >> (k & 63)) & 1ull; }
+};
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Thread 0 of each block arrives; the last to arrive resets the count and opens the next
+// generation.  `arrivals` is the number of blocks the barrier waits for (gridDim.x; more only
+// when a test makes the wait run out).  Returns false when the block must leave the kernel.
+__device__ __forceinline__ bool grid_barrier(ChunkSync *sy, unsigned int arrivals, unsigned long long budget_ns,
+                                             unsigned int index)
+{
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned int *vgen = &sy->gen;
+        volatile unsigned int *verr = &sy->error;
+        ok = 1;
+        const unsigned int g = *vgen;
+        __threadfence();
+        if (atomicAdd(&sy->count, 1u) == arrivals - 1) {
+            atomicExch(&sy->count, 0u);
+            __threadfence();
+            atomicAdd(&sy->gen, 1u);
+        } else {
+            const unsigned long long t0 = global_ns();
+            while (*vgen == g) {
+                if (*verr) {
+                    ok = 0;
+                    break;
+                }
+                if (global_ns() - t0 > budget_ns) {
+                    if (atomicExch(&sy->error, 1u) == 0u) sy->where = index;
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(100);
+            }
+        }
+        __threadfence();
+        if (*verr) ok = 0;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+template <typename R>
+__device__ __forceinline__ PackedFieldL2<R> packed_l2_of(const InstDesc &d);
+template <>
+__device__ __forceinline__ PackedFieldL2<float> packed_l2_of<float>(const InstDesc &d)
+{
+    return PackedFieldL2<float>{d.f32, d.g.V};
+}
+template <>
+__device__ __forceinline__ PackedFieldL2<double> packed_l2_of<double>(const InstDesc &d)
+{
+    return PackedFieldL2<double>{d.f64, d.g.V};
+}
+
+// nsweeps OR sweeps of every instance in want_state (a context without the separate W array:
+// plain FP64, FP32 storage, Coulomb slices with W in their temporal planes), each pass the
+// 4-lane site update of k_batched_pass, reprojecting after sweep k where repro.after(k).
+template <typename R, int GAUGE>
+__global__ void __launch_bounds__(128) k_chunk_sweeps(EngineDev e, int64_t total_warps, int64_t total_links,
+                                                      int nsweeps, ChunkReproject repro, AlgoParams p,
+                                                      int want_state, ChunkSync *sy, unsigned int arrivals,
+                                                      unsigned long long budget_ns)
+{
+    const int64_t wstride = (int64_t)gridDim.x * 4;
+    const int64_t wfirst = (int64_t)blockIdx.x * 4 + (threadIdx.x >> 5);
+    unsigned int bar = 0;
+    for (int k = 0; k < nsweeps; k++) {
+        for (int parity = 0; parity < 2; parity++) {
+            for (int64_t warp = wfirst; warp < total_warps; warp += wstride) {
+                const int i = find_instance(e.inst, e.ninst, warp, [](const InstDesc &d) { return d.warp_begin; });
+                if (e.state[i] != want_state) continue;  // warp-uniform: a tile lies in one instance
+                const InstDesc d = e.inst[i];
+                const PackedFieldL2<R> f = packed_l2_of<R>(d);
+                parity_pass_warp<R, GAUGE, ALG_OR, PackedFieldL2<R>, GAUGE == COULOMB, false>(
+                    f, f, d.g, warp - d.warp_begin, parity, p, nullptr);
+            }
+            const bool last = k == nsweeps - 1 && parity == 1 && !repro.after(k);
+            if (!last && !grid_barrier(sy, arrivals, budget_ns, bar++)) return;
+        }
+        if (repro.after(k)) {
+            for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total_links;
+                 idx += (int64_t)gridDim.x * blockDim.x) {
+                const int i = find_instance(e.inst, e.ninst, idx, [](const InstDesc &d) { return d.link_begin; });
+                if (e.state[i] != want_state) continue;
+                const InstDesc d = e.inst[i];
+                const int64_t l = idx - d.link_begin;
+                const int mu = (int)(l / d.g.V);
+                const int64_t s = l - mu * d.g.V;
+                Link<double> L;
+                load_link_f64<R>(packed_l2_of<R>(d), s, mu, L);
+                project_rows(L);
+                R o[12];
+#pragma unroll
+                for (int a = 0; a < 2; a++)
+#pragma unroll
+                    for (int b = 0; b < 3; b++) {
+                        o[2 * (3 * a + b)] = (R)L.e[a][b].x;
+                        o[2 * (3 * a + b) + 1] = (R)L.e[a][b].y;
+                    }
+                packed_of<R>(d).store12(s, mu, o);
+            }
+            if (k < nsweeps - 1 && !grid_barrier(sy, arrivals, budget_ns, bar++)) return;
+        }
+    }
+}
+
 // Quality of every instance in state want_state, with the state transitions of the check:
 //  ST_FP32 -> ST_SWITCH when theta < switch_theta (mixed runs) or when theta has stopped
 //  falling in FP32 (stall_checks), ST_FP64 -> ST_DONE when

@@ -94,6 +94,54 @@ struct PackedField<double> {
     }
 };
 
+// The packed layout read through L2 only (ld.global.cg).  A kernel that updates the field in one
+// pass and reads it in the next -- the persistent chunk kernel -- uses it: another SM may have
+// rewritten a line this SM still holds in its (non-coherent) L1 since the previous pass.
+template <typename R>
+struct PackedFieldL2;
+
+template <>
+struct PackedFieldL2<float> {
+    float4 *P;
+    int64_t V;
+    __device__ __forceinline__ void load12(int64_t s, int mu, float r[12]) const
+    {
+        const float4 *p = P + (int64_t)mu * 3 * V + s;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const float4 v = __ldcg(p + k * V);
+            r[4 * k] = v.x;
+            r[4 * k + 1] = v.y;
+            r[4 * k + 2] = v.z;
+            r[4 * k + 3] = v.w;
+        }
+    }
+    __device__ __forceinline__ void store12(int64_t s, int mu, const float r[12]) const
+    {
+        PackedField<float>{P, V}.store12(s, mu, r);
+    }
+};
+
+template <>
+struct PackedFieldL2<double> {
+    double2 *P;
+    int64_t V;
+    __device__ __forceinline__ void load12(int64_t s, int mu, double r[12]) const
+    {
+        const double2 *p = P + (int64_t)mu * 6 * V + s;
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+            const double2 v = __ldcg(p + k * V);
+            r[2 * k] = v.x;
+            r[2 * k + 1] = v.y;
+        }
+    }
+    __device__ __forceinline__ void store12(int64_t s, int mu, const double r[12]) const
+    {
+        PackedField<double>{P, V}.store12(s, mu, r);
+    }
+};
+
 template <typename R, class F>
 __device__ __forceinline__ void load_link(const F &f, int64_t s, int mu, Link<R> &L)
 {

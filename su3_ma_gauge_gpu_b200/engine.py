@@ -56,6 +56,9 @@ class Schedule:
     trace_checks: int = 0  # > 0: keep that many OR checks per instance for GaugeFixer.trace()
     fold_exit: float = 4.0  # fold mode: FP64 sweeps once the master's theta < fold_exit * precision
     rng_streams: int = 0    # 1: one Philox stream through the instances, as the apps draw it (no SR)
+    persistent: int = 0     # 1: one cooperative launch per check chunk (plain FP64, mixed=True, Coulomb)
+    wait_budget_us: int = 0  # persistent: bound of every grid-barrier wait (0: one second)
+    wait_test_missing: int = 0  # persistent: arrivals that never come (tests of the bounded wait only)
 
     @classmethod
     def mag_app(cls, **kw) -> "Schedule":

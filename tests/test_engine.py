@@ -196,7 +196,10 @@ def test_mag_app_fix_matches_oracle_driver(cuda):
     with a microcanonical sweep, per temperature, the step slowed 15x in [0.7, 0.88]), SR until
     theta < 1e-6, OR to theta < 1e-12, reprojections -- through gf_fix and through the oracle's
     restatement of apps/MAGaugeFixingSU3_4D.cu:222-333 on the same input and Philox key/counters:
-    the same sweep count in every phase, the same functional and field."""
+    the same sweep count in every phase, the same functional, and the same field up to the
+    diagonal U(1) x U(1) transformations that leave the MAG functional unchanged.  (Those are flat
+    directions: rounding differences of the two summation orders, amplified by a hundred heat-bath
+    sweeps, move the two runs apart along them, so the field is compared through |U_ij|.)"""
     from su3_ma_gauge_gpu_b200.engine import GaugeFixer, Schedule
 
     size = (4, 4, 4, 8)
@@ -218,7 +221,7 @@ def test_mag_app_fix_matches_oracle_driver(cuda):
     assert (rep.sa_sweeps, rep.sr_sweeps, rep.or_sweeps) == (r.sa_sweeps, r.sr_iterations, r.or_iterations)
     assert rep.converged and r.theta < 1e-12
     assert rep.gff == pytest.approx(r.gff, rel=1e-10)
-    assert np.abs(out - ref).max() < 1e-9
+    assert np.abs(np.abs(O.links(out, size)) - np.abs(O.links(ref, size))).max() < 1e-8
 
 
 def test_coulomb_app_fix_matches_oracle_slice_loop(cuda):
@@ -248,6 +251,89 @@ def test_coulomb_app_fix_matches_oracle_slice_loop(cuda):
         assert reps[t].converged and res[t].theta < 1e-12
         assert reps[t].gff == pytest.approx(res[t].gff, rel=1e-10), t
     assert np.abs(out - ref).max() < 1e-9
+
+
+@pytest.mark.parametrize("gauge,mixed", [("landau", False), ("landau", True), ("mag", False), ("coulomb", False)],
+                         ids=["landau-fp64", "landau-mixed", "mag-fp64", "coulomb-fp64"])
+def test_persistent_chunks_bit_identical_to_per_pass_launches(cuda, gauge, mixed):
+    """schedule.persistent = 1 runs each check chunk's sweeps and reprojections as one cooperative
+    launch with grid barriers; the fix is bit for bit the one the per-pass launches give (same
+    site update, same order), on a batch of uneven lattices, with reprojections inside chunks."""
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer
+
+    if gauge == "coulomb":
+        sizes = [(4, 4, 6, 4), (2, 8, 4, 4)]
+        fields = [np.concatenate([S.smooth_config((1,) + s[1:], 0.3, 150 + 10 * i + t)[0] for t in range(s[0])])
+                  for i, s in enumerate(sizes)]
+    else:
+        sizes = [(2, 2, 2, 6), (4, 4, 4, 4), (8, 8, 8, 8)]
+        fields = [S.smooth_config(s, 0.3, 160 + i)[0] for i, s in enumerate(sizes)]
+    outs, reps = {}, {}
+    for persistent in (0, 1):
+        with GaugeFixer(sizes, gauge=gauge, mixed=mixed) as gf:
+            gf.set_pass_shape("fp64", 0, 4)
+            if mixed:
+                gf.set_pass_shape("fp32", 0, 4)
+            for i, U in enumerate(fields):
+                gf.load(i, U)
+            reps[persistent] = gf.fix(_sched(precision=1e-12, switch_theta=1e-9, check_precision=10, reproject=7,
+                                             or_max_iter=3000, autotune=0, persistent=persistent))
+            outs[persistent] = []
+            for i, U in enumerate(fields):
+                o = np.zeros_like(U)
+                gf.store(i, o)
+                outs[persistent].append(o)
+    for a, b in zip(reps[0], reps[1]):
+        assert (a.gff, a.theta, a.or_sweeps, a.or_sweeps_fp64) == (b.gff, b.theta, b.or_sweeps, b.or_sweeps_fp64)
+        assert b.converged
+    for a, b in zip(outs[0], outs[1]):
+        assert np.array_equal(a, b)
+
+
+def test_persistent_chunk_wait_runs_out_and_reports_timeout(cuda):
+    """Every grid-barrier wait of the persistent chunk kernel is bounded.  With a barrier that waits
+    for one arrival that never comes, every block gives up after the budget (2 ms), the kernel
+    returns, and gf_fix reports GF_ERR_TIMEOUT; the context stays usable and the next fix on a
+    reloaded field converges to the per-pass result."""
+    from su3_ma_gauge_gpu_b200 import _lib
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer
+
+    size = (8, 8, 8, 8)
+    U, _ = S.smooth_config(size, 0.3, 170)
+    with GaugeFixer([size], mixed=False) as gf:
+        gf.load(0, U)
+        with pytest.raises(_lib.GaugeFixError) as err:
+            gf.fix(_sched(precision=1e-12, check_precision=10, persistent=1, wait_budget_us=2000, wait_test_missing=1))
+        assert err.value.status == _lib.GF_ERR_TIMEOUT
+        assert "ran out" in str(err.value)
+        gf.load(0, U)
+        rep = gf.fix(_sched(precision=1e-12, check_precision=10, persistent=1))[0]
+    with GaugeFixer([size], mixed=False) as gf:
+        gf.load(0, U)
+        ref = gf.fix(_sched(precision=1e-12, check_precision=10))[0]
+    assert rep.converged and rep.gff == pytest.approx(ref.gff, rel=1e-13) and rep.or_sweeps == ref.or_sweeps
+
+
+def test_check_chunk_graphs_are_kept_across_fixes(cuda):
+    """The captured check-chunk graphs belong to the context: a second gf_fix with the same schedule
+    replays them (same launches counted, same result), and changing the launch shape drops them."""
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer
+
+    size = (4, 4, 4, 8)
+    U, _ = S.smooth_config(size, 0.3, 171)
+    with GaugeFixer([size], mixed=False) as gf:
+        gf.set_pass_shape("fp64", 0, 4)
+        res = []
+        for _ in range(2):
+            gf.load(0, U)
+            l0 = gf.kernel_launches()
+            res.append((gf.fix(_sched(precision=1e-12, check_precision=10, autotune=0))[0], gf.kernel_launches() - l0))
+        gf.set_pass_shape("fp64", 1, 4)
+        gf.load(0, U)
+        third = gf.fix(_sched(precision=1e-12, check_precision=10, autotune=0))[0]
+    (a, na), (b, nb) = res
+    assert (a.gff, a.or_sweeps) == (b.gff, b.or_sweeps) and na == nb
+    assert third.gff == a.gff and third.or_sweeps == a.or_sweeps
 
 
 def _mixed_vs_fp64(size, eps, seed):
@@ -375,7 +461,9 @@ def test_two_lane_pass_matches_direct(cuda, gauge, algo, prec):
                 gf.store(i, o)
                 res.append(o)
             outs.append(res)
-    tol = 1e-13 if prec == "fp64" else (1e-4 if (gauge, algo) == ("u1xu1", "micro") else 1e-5)
+    # U1xU1 micro and SR steps normalise a two-component quaternion that is small at some sites of a
+    # Haar-transformed field: there one FP32 rounding difference grows to a few 1e-5
+    tol = 1e-13 if prec == "fp64" else (1e-4 if (gauge, algo) in (("u1xu1", "micro"), ("u1xu1", "sr")) else 1e-5)
     for a, b in zip(*outs):
         assert np.abs(a - b).max() < tol
 
