@@ -48,6 +48,8 @@ BYTES_PER_SITE_UPDATE = {"fp32": 768, "fp64": 1536, "fp32_refine": 768 + 96}
 
 def pass_kernel_name(code: int, real: str, refine: bool) -> str:
     """The OR-pass kernel an autotuner choice stands for (gf_autotune's output codes)."""
+    if code >= 1000:
+        return pass_kernel_name(code - 1000, real, refine) + ", odd-parity passes walked backwards"
     r = "float" if real == "fp32" else "double"
     w = ", W" if refine and real == "fp32" else ""
     if code == 100:

@@ -101,6 +101,7 @@ struct gf_ctx {
     // tile), `warps` warps per block, grid = num_sms * blocks_per_sm
     struct PassShape {
         int variant = 0, warps = 4, blocks_per_sm = 0;
+        int alternate = 0;  // persistent variants (1, 3, 7): walk the tiles backwards on odd parities
     } shape[2];
     int tuned[2] = {0, 0};
     // the lattices the caller passed: first instance and number of instances (Coulomb contexts
@@ -145,6 +146,7 @@ struct PassArgs {
     int parity;
     AlgoParams p;
     int want_state;
+    int reverse;  // persistent passes: walk the tiles backwards
 };
 
 template <typename R, int GAUGE, int ALGO, int WARPS>
@@ -167,7 +169,7 @@ int launch_staged(const gf_ctx *c, const EngineDev &e, const PassArgs &a, int bl
     }
     const int64_t need = (a.c->total_warps + WARPS - 1) / WARPS;
     const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)c->num_sms * occ));
-    kern<<<blocks, WARPS * 32, smem, a.c->stream>>>(e, a.c->total_warps, a.parity, a.p, a.want_state);
+    kern<<<blocks, WARPS * 32, smem, a.c->stream>>>(e, a.c->total_warps, a.parity, a.p, a.want_state, a.reverse);
     return launch_status("batched parity pass (pipelined)");
 }
 
@@ -187,7 +189,7 @@ int launch_rp(const gf_ctx *c, const EngineDev &e, const PassArgs &a, int blocks
     }
     const int64_t need = (a.c->total_warps + 3) / 4;
     const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)c->num_sms * occ));
-    kern<<<blocks, 128, 0, a.c->stream>>>(e, a.c->total_warps, a.parity, a.p, a.want_state);
+    kern<<<blocks, 128, 0, a.c->stream>>>(e, a.c->total_warps, a.parity, a.p, a.want_state, a.reverse);
     return launch_status("batched parity pass (register prefetch)");
 }
 
@@ -228,7 +230,7 @@ int launch_pair_rp(const gf_ctx *c, const EngineDev &e, const PassArgs &a, int b
     }
     const int64_t need = ((a.c->total_warps + 1) / 2 + 3) / 4;  // 16-site pair tiles, 4 warps per block
     const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)c->num_sms * occ));
-    kern<<<blocks, 128, 0, a.c->stream>>>(e, a.c->total_warps, a.parity, a.p, a.want_state);
+    kern<<<blocks, 128, 0, a.c->stream>>>(e, a.c->total_warps, a.parity, a.p, a.want_state, a.reverse);
     return launch_status("batched parity pass (two lanes per site, register prefetch)");
 }
 
@@ -330,8 +332,9 @@ int launch_sweep_on(const gf_ctx *c, const EngineDev &e, const gf_ctx::PassShape
                     float param, uint32_t seed, uint32_t counter_even, uint32_t counter_odd)
 {
     for (int parity = 0; parity < 2; parity++) {
+        const gf_ctx::PassShape &sh = shape[want_state == ST_FP32 ? 0 : 1];
         PassArgs a{c, parity, AlgoParams{param, seed, parity ? counter_odd : counter_even, c->counter_stride},
-                   want_state};
+                   want_state, sh.alternate && parity == 1};
         int st = dispatch_gauge_algo<BatchedPass>(c->gauge, algo, a, e, shape);
         if (st) return st;
         c->launches++;
@@ -1251,15 +1254,17 @@ int gf_autotune(gf_ctx *c, int *choice_fp32, int *choice_fp64)
     // prefetch); pipelined with 2, 4, 8 warps per block; (FP32 only) direct capped at 64 registers and
     // one thread per site (plain and pipelined).  Coulomb passes are direct only; refine-FP32 passes
     // (W tracking) are not the 4-lane pipelined one.
-    static const gf_ctx::PassShape cands64[] = {{0, 4, 0}, {3, 4, 0}, {6, 4, 0}, {1, 2, 0}, {1, 4, 0}, {1, 8, 0}};
-    static const gf_ctx::PassShape cands32[] = {{0, 4, 0}, {2, 4, 0}, {3, 4, 0}, {4, 4, 0}, {5, 4, 0},
-                                                {6, 4, 0}, {7, 4, 0}, {1, 2, 0}, {1, 4, 0}, {1, 8, 0}};
+    static const gf_ctx::PassShape cands64[] = {{0, 4, 0, 0}, {3, 4, 0, 0}, {6, 4, 0, 0}, {1, 4, 0, 1}, {1, 8, 0, 1},
+                                                {3, 4, 0, 1}, {1, 2, 0, 0}, {1, 4, 0, 0}, {1, 8, 0, 0}};
+    static const gf_ctx::PassShape cands32[] = {{0, 4, 0, 0}, {2, 4, 0, 0}, {3, 4, 0, 0}, {4, 4, 0, 0}, {5, 4, 0, 0},
+                                                {6, 4, 0, 0}, {7, 4, 0, 0}, {7, 4, 0, 1}, {3, 4, 0, 1},
+                                                {1, 2, 0, 0}, {1, 4, 0, 0}, {1, 8, 0, 0}};
     for (int prec = 0; prec < 2; prec++) {
         if (prec == 0 && !c->mixed) continue;
         const gf_ctx::PassShape *cands = prec == 0 ? cands32 : cands64;
-        int ncand = prec == 0 ? 10 : 6;
+        int ncand = prec == 0 ? 12 : 9;
         if (c->gauge == GF_COULOMB) ncand = 1;
-        else if (prec == 0 && c->site_w) ncand = 7;
+        else if (prec == 0 && c->site_w) ncand = 9;
         // scratch field, descriptors and states for this precision
         const InstDesc &last = c->h_inst.back();
         const size_t span32 = (size_t)(reinterpret_cast<const char *>(last.f32 ? last.f32 : (float4 *)nullptr) -
@@ -1345,14 +1350,14 @@ int gf_autotune(gf_ctx *c, int *choice_fp32, int *choice_fp64)
         c->drop_graphs();
     }
     auto code = [](const gf_ctx::PassShape &sh) {
-        return sh.variant == 1 ? sh.warps
+        return (sh.alternate ? 1000 : 0) + (sh.variant == 1 ? sh.warps
                : sh.variant == 2 ? 64
                : sh.variant == 3 ? 100
                : sh.variant == 4 ? 32
                : sh.variant == 5 ? 33
                : sh.variant == 6 ? 16
                : sh.variant == 7 ? 116
-                                 : 0;
+                                 : 0);
     };
     if (choice_fp32) *choice_fp32 = c->mixed ? code(c->shape[0]) : -1;
     if (choice_fp64) *choice_fp64 = code(c->shape[1]);
@@ -1377,8 +1382,23 @@ int gf_set_pass_shape(gf_ctx *c, int real, int variant, int warps)
     c->drop_graphs();
     c->shape[real].variant = variant;
     c->shape[real].warps = warps;
+    c->shape[real].alternate = 0;
     c->shape[real].blocks_per_sm = 0;
     c->tuned[real] = 1;
+    return GF_OK;
+}
+
+// Walk order of the persistent parity passes (variants 1, 3 and 7): alternate = 1 walks the tiles of
+// odd-parity passes backwards, so every pass starts on the links the previous one touched last.
+int gf_set_pass_order(gf_ctx *c, int real, int alternate)
+{
+    clear_error();
+    if (!c || !valid_real(real) || (alternate != 0 && alternate != 1)) {
+        set_error("invalid argument to gf_set_pass_order");
+        return GF_ERR_INVALID;
+    }
+    c->drop_graphs();
+    c->shape[real].alternate = alternate;
     return GF_OK;
 }
 

@@ -46,6 +46,11 @@ struct EngineDev {
     int trace_cap;
 };
 
+// Traversal order of a persistent pass: with `reverse` the tiles are walked from the last to the
+// first.  Consecutive parity passes alternate direction, so a pass starts where the previous one
+// ended, on the links still held in L2 (every pass touches every link once).
+__device__ __forceinline__ int64_t ordered_tile(int64_t t, int64_t n, int reverse) { return reverse ? n - 1 - t : t; }
+
 // index of the instance whose range [begin[i], begin[i+1]) holds x (ranges ascending)
 template <typename F>
 __device__ __forceinline__ int find_instance(const InstDesc *inst, int n, int64_t x, F begin_of)
@@ -180,7 +185,7 @@ __device__ __forceinline__ void fetch_tile_regs(const EngineDev &e, const InstCa
 
 template <typename R, int GAUGE, int ALGO, bool SITE_W>
 __global__ void __launch_bounds__(128) k_batched_pass_rp(EngineDev e, int64_t total_warps, int parity, AlgoParams p,
-                                                         int want_state)
+                                                         int want_state, int reverse)
 {
     static_assert(GAUGE != COULOMB, "Coulomb slices use k_batched_pass");
     __shared__ InstCache ic;
@@ -190,11 +195,14 @@ __global__ void __launch_bounds__(128) k_batched_pass_rp(EngineDev e, int64_t to
     int64_t tile = (int64_t)blockIdx.x * 4 + (threadIdx.x >> 5);
     TileRegs<R> cur;
     cur.inst = -1;
-    if (tile < total_warps) fetch_tile_regs<R, SITE_W>(e, ic, tile, parity, want_state, cur);
+    if (tile < total_warps)
+        fetch_tile_regs<R, SITE_W>(e, ic, ordered_tile(tile, total_warps, reverse), parity, want_state, cur);
     for (; tile < total_warps; tile += stride) {
         TileRegs<R> nxt;
         nxt.inst = -1;
-        if (tile + stride < total_warps) fetch_tile_regs<R, SITE_W>(e, ic, tile + stride, parity, want_state, nxt);
+        if (tile + stride < total_warps)
+            fetch_tile_regs<R, SITE_W>(e, ic, ordered_tile(tile + stride, total_warps, reverse), parity, want_state,
+                                       nxt);
         if (cur.inst >= 0) {
             const InstDesc &d = inst_at(e, ic, cur.inst);
             Link<R> up, dn;
@@ -420,7 +428,7 @@ __device__ __forceinline__ void fetch_pair_regs(const EngineDev &e, const InstCa
 
 template <typename R, int GAUGE, int ALGO, bool SITE_W>
 __global__ void __launch_bounds__(128) k_batched_pass_pair_rp(EngineDev e, int64_t total_tiles, int parity,
-                                                              AlgoParams p, int want_state)
+                                                              AlgoParams p, int want_state, int reverse)
 {
     static_assert(GAUGE != COULOMB, "Coulomb slices use k_batched_pass");
     __shared__ InstCache ic;
@@ -430,11 +438,17 @@ __global__ void __launch_bounds__(128) k_batched_pass_pair_rp(EngineDev e, int64
     const int64_t stride = (int64_t)gridDim.x * 4;
     int64_t pt = (int64_t)blockIdx.x * 4 + (threadIdx.x >> 5);   // this warp's pair tile
     PairRegs<R> cur;
-    fetch_pair_regs<R, SITE_W>(e, ic, pt * 2 + half, total_tiles, parity, want_state, cur);
+    cur.ps.inst = -1;
+    if (pt < npair)
+        fetch_pair_regs<R, SITE_W>(e, ic, ordered_tile(pt, npair, reverse) * 2 + half, total_tiles, parity, want_state,
+                                   cur);
     // every lane of a warp runs the same iterations (pt is warp-uniform), so the shuffles are safe
     for (; pt < npair; pt += stride) {
         PairRegs<R> nxt;
-        fetch_pair_regs<R, SITE_W>(e, ic, (pt + stride) * 2 + half, total_tiles, parity, want_state, nxt);
+        nxt.ps.inst = -1;
+        if (pt + stride < npair)
+            fetch_pair_regs<R, SITE_W>(e, ic, ordered_tile(pt + stride, npair, reverse) * 2 + half, total_tiles, parity,
+                                       want_state, nxt);
         const int i = cur.ps.inst;
         if (__any_sync(0xffffffffu, i >= 0)) {
             Link<R> up[2], dn[2];
@@ -885,7 +899,7 @@ __device__ __forceinline__ void unstage_link(const uint4 *stage, int first, Link
 
 template <typename R, int GAUGE, int ALGO, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32) k_batched_pass_staged(EngineDev e, int64_t total_warps, int parity,
-                                                                      AlgoParams p, int want_state)
+                                                                      AlgoParams p, int want_state, int reverse)
 {
     extern __shared__ uint4 smem[];
     constexpr int NCH = Chunks<R>::per_lane;
@@ -894,11 +908,14 @@ __global__ void __launch_bounds__(WARPS * 32) k_batched_pass_staged(EngineDev e,
     const int64_t stride = (int64_t)gridDim.x * WARPS;
     int64_t tile = (int64_t)blockIdx.x * WARPS + w;
     int cur = 0;
-    TileRef t = tile < total_warps ? prefetch_tile<R>(e, tile, parity, want_state, wbase) : TileRef{-1, 0, 0, 0};
+    TileRef t = tile < total_warps ? prefetch_tile<R>(e, ordered_tile(tile, total_warps, reverse), parity, want_state,
+                                                      wbase)
+                                   : TileRef{-1, 0, 0, 0};
     cp_async_commit();
     for (; tile < total_warps; tile += stride) {
         const int64_t nt = tile + stride;
-        const TileRef n = nt < total_warps ? prefetch_tile<R>(e, nt, parity, want_state, wbase + (cur ^ 1) * NCH * 32)
+        const TileRef n = nt < total_warps ? prefetch_tile<R>(e, ordered_tile(nt, total_warps, reverse), parity,
+                                                              want_state, wbase + (cur ^ 1) * NCH * 32)
                                            : TileRef{-1, 0, 0, 0};
         cp_async_commit();
         cp_async_wait<1>();

@@ -382,13 +382,17 @@ def test_pipelined_pass_bit_identical_to_direct(cuda, prec):
     mixed = {"fp32": True, "fp64": False, "refine": "refine"}[prec]
     outs = {}
     if prec == "refine":
-        shapes = [(0, 4), (2, 4), (3, 4), (4, 4), (5, 4), (6, 4), (7, 4)]
+        shapes = [(0, 4), (2, 4), (3, 4), (4, 4), (5, 4), (6, 4), (7, 4), (7, 4, 1), (3, 4, 1)]
     else:
-        shapes = [(0, 4), (1, 2), (1, 4), (1, 8), (3, 4), (6, 4)] + ([(2, 4), (4, 4), (5, 4), (7, 4)]
-                                                                     if prec == "fp32" else [])
-    for variant, warps in shapes:
+        shapes = [(0, 4), (1, 2), (1, 4), (1, 8), (3, 4), (6, 4), (1, 4, 1), (1, 8, 1), (3, 4, 1)] + (
+            [(2, 4), (4, 4), (5, 4), (7, 4), (7, 4, 1)] if prec == "fp32" else [])
+    for shape in shapes:
+        variant, warps = shape[:2]
         with GaugeFixer(sizes, mixed=mixed) as gf:
-            gf.set_pass_shape("fp64" if prec == "fp64" else "fp32", variant, warps)
+            real = "fp64" if prec == "fp64" else "fp32"
+            gf.set_pass_shape(real, variant, warps)
+            if len(shape) > 2:
+                gf.set_pass_order(real, True)
             for i, U in enumerate(fields):
                 gf.load(i, U)
             gf.sweeps("or", 4, 1.7)
@@ -397,7 +401,7 @@ def test_pipelined_pass_bit_identical_to_direct(cuda, prec):
                 o = np.zeros_like(U)
                 gf.store(i, o)
                 res.append(o)
-            outs[(variant, warps)] = res
+            outs[shape] = res
     base = outs[(0, 4)]
     for key, res in outs.items():
         for i in range(len(sizes)):
