@@ -239,6 +239,11 @@ int gf_import(gf_ctx *ctx, int lattice, int real, const void *U, int on_host);
 /* Write lattice `lattice` back in the same layout, reunitarised in FP64 with row 2 rebuilt
  * (the reference's closing projectSU3, apps/LandauGaugeFixingSU3_4D.cu:271). */
 int gf_export(gf_ctx *ctx, int lattice, int real, void *U, int on_host);
+/* GF_COULOMB contexts holding gauge copies of one configuration (one lattice per copy): write the
+ * lattice whose timeslice t is that of copy copy_of_slice[t] -- the best copy of every timeslice,
+ * as apps/CoulombGaugeFixingSU3_4D.cu:303-311 keeps it -- with temporal links
+ * W_a(t) U_0(t) W_b(t+1)^dagger for a = copy_of_slice[t], b = copy_of_slice[t+1]. */
+int gf_export_slices(gf_ctx *ctx, const int *copy_of_slice, int real, void *U, int on_host);
 /* nsweeps full sweeps (both parities) of one algorithm (0 OR, 1 micro, 2 SA, 3 SR, 4 random
  * trafo) on every instance still sweeping; Philox counters rng_counter, rng_counter+1, ... */
 int gf_sweeps(gf_ctx *ctx, int algo, int nsweeps, float param, int seed, int rng_counter);

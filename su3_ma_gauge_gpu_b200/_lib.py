@@ -94,6 +94,7 @@ SIGNATURES.update({
     "gf_destroy": (_c_int, [_vp]),
     "gf_import": (_c_int, [_vp, _c_int, _c_int, _vp, _c_int]),
     "gf_export": (_c_int, [_vp, _c_int, _c_int, _vp, _c_int]),
+    "gf_export_slices": (_c_int, [_vp, ctypes.POINTER(_c_int), _c_int, _vp, _c_int]),
     "gf_sweeps": (_c_int, [_vp, _c_int, _c_int, _c_float, _c_int, _c_int]),
     "gf_quality_all": (_c_int, [_vp, _dp, _dp]),
     "gf_reunitarize": (_c_int, [_vp]),

@@ -11,11 +11,22 @@ together (every parity pass is one launch over all copies, convergence per copy 
 and the file I/O is the GPU transcoder.  Options keep the reference's names and defaults
 (apps/program_options/ProgramOptions.hxx:223-266).
 
-Differences, stated: copy c draws its random gauge transformation and SA heat-bath numbers from
-Philox key word seed + c (the reference advances one global counter across copies); the
-precision is compared as a float, like the reference's ``float precision``; for GF_COULOMB the
-lattice's timeslices are fixed together and one copy is supported (the reference keeps the best
-copy per timeslice).
+Gauge copies run in one of two ways (``copies=``):
+
+* ``"batched"`` (default): all copies of a configuration are instances of ONE context, fixed
+  together from the same input; copy c draws its random gauge transformation and heat-bath numbers
+  from Philox key word seed + c.  For GF_COULOMB every copy is a lattice of Nt timeslices, and the
+  written configuration takes, timeslice by timeslice, the copy with the largest functional of that
+  slice (gf_export_slices) -- the rule of apps/CoulombGaugeFixingSU3_4D.cu:303-311.
+* ``"reference"``: the apps' own sequence (apps/LandauGaugeFixingSU3_4D.cu:184-283,
+  apps/MAGaugeFixingSU3_4D.cu:197-373): copies one after the other, each starting from the best
+  copy found so far (the apps reload their host array, which holds it), one Philox counter running
+  on through the random transformations, SA and SR sweeps of all copies (PhiloxWrapper's
+  process-wide counter, lattice/rng/PhiloxWrapper.hxx:90,142-145), a hot start drawing counter 0.
+  For GF_COULOMB with one copy this is the batched fix with ``rng_streams = 1``, which gives every
+  timeslice the key word and counters of the app's slice loop; several Coulomb copies run batched.
+
+The precision is compared as a float, like the reference's ``float precision``.
 """
 from __future__ import annotations
 
@@ -130,26 +141,26 @@ def schedule_for(gauge: str, o: ProgramOptions, **extra) -> Schedule:
 @dataclass
 class ConfigResult:
     filename: str
-    functionals: list      # per copy (per timeslice for Coulomb)
+    functionals: list      # per copy (Coulomb: the mean over the copy's timeslices)
     thetas: list
     best_copy: int
     output: str | None
 
 
-def run(gauge: str, size, options: ProgramOptions, mixed=False, precision="double", **schedule_extra):
+def run(gauge: str, size, options: ProgramOptions, mixed=False, precision="double", copies="batched",
+        **schedule_extra):
     """Fix every configuration of the FileIterator with `gaugecopies` copies each; writes the
-    per-copy functional CSV ("copy,functional", 17 digits) and the best copy (or, with save_each,
-    every improving copy but the last as <output>_<copy+1>, then the best).  Returns one
-    ConfigResult per file."""
+    per-copy functional CSV ("copy,functional", 17 digits; Coulomb: "copy,timeslice,functional") and
+    the best copy (or, with save_each, every improving copy but the last as <output>_<copy+1>, then
+    the best).  Returns one ConfigResult per file."""
+    if copies not in ("batched", "reference"):
+        raise ValueError("copies must be 'batched' or 'reference'")
     size = tuple(int(v) for v in size)
-    copies = max(1, int(options.gaugecopies))
-    if gauge == "coulomb" and copies != 1:
-        raise ValueError("Coulomb: one gauge copy per configuration (the timeslices are fixed together)")
+    ncopies = max(1, int(options.gaugecopies))
     layout = "timeslice" if gauge == "coulomb" else "gpu"
     dtype = np.float64 if precision in ("double", "fp64") else np.float32
     it = FileIterator(options)
     out = []
-    sched = schedule_for(gauge, options, **schedule_extra)
     for i in it.ids():
         fname = it.filename(i)
         U = np.zeros(72 * int(np.prod(size)), dtype=dtype)
@@ -162,31 +173,97 @@ def run(gauge: str, size, options: ProgramOptions, mixed=False, precision="doubl
             U = dU.cpu().numpy()
         else:
             files.read_config(fname, options.ftype, size, U, precision, options.reinterpret, layout=layout)
-        with GaugeFixer([size] * copies, gauge=gauge, mixed=mixed) as gf:
-            for c in range(copies):
-                gf.load(c, U)
-            gf.fix(sched)
-            g, a = gf.quality()
-            results = []
-            for c in range(copies):
-                R = np.zeros_like(U)
-                gf.store(c, R)
-                results.append(R)
-        lines = ["copy,functional"] + [f"{c},{g[c]:.17g}" for c in range(len(g))]
+        if gauge == "coulomb":
+            res = _coulomb_copies(size, options, U, mixed, ncopies, copies, schedule_extra)
+        elif copies == "reference":
+            res = _sequential_copies(gauge, size, options, U, mixed, ncopies, schedule_extra)
+        else:
+            res = _batched_copies(gauge, size, options, U, mixed, ncopies, schedule_extra)
+        functionals, thetas, fields, best, best_field, lines = res
         Path(it.output_functional(i)).write_text("\n".join(lines) + "\n")
-        best, bestF = 0, -np.inf
         outname = None
-        for c in range(copies):
-            if g[c] > bestF:
-                bestF, best = g[c], c
-                if options.save_each and c < copies - 1 and not options.hotgaugefield:
-                    _save(gauge, size, options, precision, fname, f"{it.output_filename(i)}_{c + 1}", results[c],
-                          layout)
-        if not options.hotgaugefield and not options.save_each:
+        if options.save_each and not options.hotgaugefield:
+            bestF = -np.inf
+            for c in range(ncopies):
+                if functionals[c] > bestF:
+                    bestF = functionals[c]
+                    if c < ncopies - 1:
+                        _save(gauge, size, options, precision, fname, f"{it.output_filename(i)}_{c + 1}", fields[c],
+                              layout)
+        elif not options.hotgaugefield:
             outname = it.output_filename(i)
-            _save(gauge, size, options, precision, fname, outname, results[best], layout)
-        out.append(ConfigResult(fname, list(g), list(a), best, outname))
+            _save(gauge, size, options, precision, fname, outname, best_field, layout)
+        out.append(ConfigResult(fname, list(functionals), list(thetas), best, outname))
     return out
+
+
+def _export(gf, c, U):
+    R = np.zeros_like(U)
+    gf.store(c, R)
+    return R
+
+
+def _batched_copies(gauge, size, options, U, mixed, ncopies, extra):
+    sched = schedule_for(gauge, options, **extra)
+    with GaugeFixer([size] * ncopies, gauge=gauge, mixed=mixed) as gf:
+        for c in range(ncopies):
+            gf.load(c, U)
+        gf.fix(sched)
+        g, a = gf.quality()
+        fields = [_export(gf, c, U) for c in range(ncopies)]
+    best = int(np.argmax(g))  # the first of equal maxima, as the apps' strict '>'
+    lines = ["copy,functional"] + [f"{c},{g[c]:.17g}" for c in range(ncopies)]
+    return list(g), list(a), fields, best, fields[best], lines
+
+
+def _sequential_copies(gauge, size, options, U, mixed, ncopies, extra):
+    """The apps' copy loop: each copy from the best so far, one counter through all copies."""
+    counter = 1 if options.hotgaugefield else 0  # setHot drew counter 0
+    start = U.copy()
+    best_f, best = 0.0, 0
+    best_field = U
+    g_all, a_all, fields = [], [], []
+    with GaugeFixer([size], gauge=gauge, mixed=mixed) as gf:
+        gf.load(0, start)
+        for c in range(ncopies):
+            if not options.hotgaugefield:
+                gf.load(0, start)  # the apps copy their host array, which holds the best copy so far
+            sched = schedule_for(gauge, options, rng_counter=counter, **extra)
+            rep = gf.fix(sched)[0]
+            counter += 2 * sched.random_trafo + 2 * rep.sa_sweeps + 2 * rep.sr_sweeps
+            R = _export(gf, 0, U)
+            g_all.append(rep.gff)
+            a_all.append(rep.theta)
+            fields.append(R)
+            if rep.gff > best_f:
+                best_f, best, best_field = rep.gff, c, R
+                start = R
+    lines = ["copy,functional"] + [f"{c},{g_all[c]:.17g}" for c in range(ncopies)]
+    return g_all, a_all, fields, best, best_field, lines
+
+
+def _coulomb_copies(size, options, U, mixed, ncopies, copies, extra):
+    """Coulomb: every copy a lattice of Nt timeslices in one context; the written configuration takes
+    each timeslice from its best copy (gf_export_slices).  One copy in "reference" mode draws the
+    app's Philox stream slice by slice (rng_streams = 1)."""
+    nt = size[0]
+    if copies == "reference" and ncopies == 1:
+        extra = dict(extra, rng_streams=1)
+    sched = schedule_for("coulomb", options, **extra)
+    with GaugeFixer([size] * ncopies, gauge="coulomb", mixed=mixed) as gf:
+        for c in range(ncopies):
+            gf.load(c, U)
+        gf.fix(sched)
+        g, a = gf.quality()
+        g = np.asarray(g).reshape(ncopies, nt)
+        a = np.asarray(a).reshape(ncopies, nt)
+        fields = [_export(gf, c, U) for c in range(ncopies)]
+        pick = [int(np.argmax(g[:, t])) for t in range(nt)]
+        best_field = np.zeros_like(U)
+        gf.store_slices(pick, best_field)
+    lines = ["copy,timeslice,functional"] + [f"{c},{t},{g[c, t]:.17g}" for c in range(ncopies) for t in range(nt)]
+    per_copy = list(g.mean(axis=1))
+    return per_copy, list(a.max(axis=1)), fields, int(np.argmax(per_copy)), best_field, lines
 
 
 def _save(gauge, size, options, precision, template, outname, U, layout):

@@ -820,9 +820,9 @@ int gf_export(gf_ctx *c, int lat, int real, void *U, int on_host)
         void *dp = dst + (size_t)t * L.slice_reals * es;
         if (c->gauge == GF_COULOMB) {
             if (real == GF_FP64)
-                k_export_coulomb<double><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (double *)dp, c->refine);
+                k_export_coulomb<double><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (double *)dp, c->refine, -1);
             else
-                k_export_coulomb<float><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (float *)dp, c->refine);
+                k_export_coulomb<float><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (float *)dp, c->refine, -1);
         } else if (c->h_state[c->ninst + i] == 0 && c->refine) {
             if (real == GF_FP64) k_export_refine<double><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (double *)dp);
             else k_export_refine<float><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (float *)dp);
@@ -838,6 +838,57 @@ int gf_export(gf_ctx *c, int lat, int real, void *U, int on_host)
     }
     if (on_host && (st = cuda_status(cudaMemcpyAsync(U, dst, (size_t)L.slice_reals * L.count * es,
                                                      cudaMemcpyDeviceToHost, c->stream), "D2H")))
+        return st;
+    return cuda_status(cudaStreamSynchronize(c->stream), "export sync");
+}
+
+// Coulomb gauge copies: export one lattice made of the timeslices of several copies -- slice t from
+// lattice copy_of_slice[t] -- as the Coulomb app keeps the best copy of every timeslice
+// (apps/CoulombGaugeFixingSU3_4D.cu:303-311).  Spatial links of slice t are copy a_t's; the temporal
+// links are W_{a_t}(t) U_0(t) W_{a_{t+1}}(t+1)^dagger, which is what the app's slice-by-slice
+// multiplications produce when slice t's best copy is a_t.  Every lattice must have the extents
+// of the first; the copies must have been imported from the same configuration.
+int gf_export_slices(gf_ctx *c, const int *copy_of_slice, int real, void *U, int on_host)
+{
+    clear_error();
+    int st = check_ctx(c);
+    if (st) return st;
+    if (c->gauge != GF_COULOMB || !copy_of_slice || !U || !valid_real(real)) {
+        set_error("gf_export_slices: a GF_COULOMB context, a slice-to-copy table and a field are needed");
+        return GF_ERR_INVALID;
+    }
+    const gf_ctx::Lattice &L0 = c->lattices[0];
+    const int nt = L0.count;
+    for (int t = 0; t < nt; t++) {
+        const int a = copy_of_slice[t];
+        if (a < 0 || a >= (int)c->lattices.size() || c->lattices[a].count != nt ||
+            c->lattices[a].slice_reals != L0.slice_reals ||
+            std::memcmp(c->h_inst[c->lattices[a].first].g.n, c->h_inst[L0.first].g.n, sizeof(int32_t) * 4) != 0) {
+            set_error("gf_export_slices: slice %d names copy %d, which is not a lattice of the same extents", t, a);
+            return GF_ERR_INVALID;
+        }
+    }
+    const size_t es = real == GF_FP64 ? 8 : 4;
+    if ((st = sync_states(c))) return st;
+    char *dst = (char *)U;
+    if (on_host) {
+        if ((st = ensure_staging(c, (size_t)L0.slice_reals * nt * es))) return st;
+        dst = (char *)c->staging;
+    }
+    for (int t = 0; t < nt; t++) {
+        const int i = c->lattices[copy_of_slice[t]].first + t;
+        const int next = c->lattices[copy_of_slice[(t + 1) % nt]].first + (t + 1) % nt;
+        const unsigned blocks = grid_for(4 * c->h_inst[i].g.V, 256);
+        void *dp = dst + (size_t)t * L0.slice_reals * es;
+        if (real == GF_FP64)
+            k_export_coulomb<double><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (double *)dp, c->refine, next);
+        else
+            k_export_coulomb<float><<<blocks, 256, 0, c->stream>>>(c->dev(), i, (float *)dp, c->refine, next);
+        c->launches++;
+        if ((st = launch_status("export slices"))) return st;
+    }
+    if (on_host && (st = cuda_status(cudaMemcpyAsync(U, dst, (size_t)L0.slice_reals * nt * es, cudaMemcpyDeviceToHost,
+                                                     c->stream), "D2H")))
         return st;
     return cuda_status(cudaStreamSynchronize(c->stream), "export sync");
 }

@@ -1398,9 +1398,11 @@ __device__ __forceinline__ void coulomb_w_total(const EngineDev &e, int i, int64
 
 // Coulomb export of timeslice i: spatial links as k_export (a refine slice whose working copy is
 // current exports its master with W32 applied); temporal links
-// U_0(t,x) <- W(t,x) U_0(t,x) W(t+1,x)^dagger, W read from each slice's current storage.
+// U_0(t,x) <- W(t,x) U_0(t,x) W(t+1,x)^dagger, W read from each slice's current storage; W(t+1) is
+// that of instance `next` when next >= 0 (slice t+1 taken from another gauge copy), else of the
+// lattice's own slice t+1.
 template <typename Rout>
-__global__ void __launch_bounds__(256) k_export_coulomb(EngineDev e, int i, Rout *U, int refine)
+__global__ void __launch_bounds__(256) k_export_coulomb(EngineDev e, int i, Rout *U, int refine, int next)
 {
     const InstDesc d = e.inst[i];
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1416,7 +1418,7 @@ __global__ void __launch_bounds__(256) k_export_coulomb(EngineDev e, int i, Rout
     } else {
         Link<double> W, Wn, T;
         coulomb_w_total(e, i, s, refine != 0, W);
-        coulomb_w_total(e, d.next, s, refine != 0, Wn);
+        coulomb_w_total(e, next >= 0 ? next : d.next, s, refine != 0, Wn);
         load_link_f64<double>(PackedField<double>{d.t64, d.g.V}, s, 0, T);
         Link<double> M;  // W T
         mul33(W, T, M);

@@ -148,6 +148,15 @@ class GaugeFixer:
         else:
             check(lib().gf_export(self._h, i, _real(U), U.data_ptr(), 0), "gf_export")
 
+    def store_slices(self, copy_of_slice, U) -> None:
+        """Coulomb gauge copies: export the lattice whose timeslice t comes from copy copy_of_slice[t]."""
+        tab = (ctypes.c_int * len(copy_of_slice))(*[int(a) for a in copy_of_slice])
+        if isinstance(U, np.ndarray):
+            assert U.flags.c_contiguous
+            check(lib().gf_export_slices(self._h, tab, _real(U), U.ctypes.data, 1), "gf_export_slices")
+        else:
+            check(lib().gf_export_slices(self._h, tab, _real(U), U.data_ptr(), 0), "gf_export_slices")
+
     def sweeps(self, algo: str, n: int, param: float = 0.0, seed: int = 0, rng_counter: int = 0) -> None:
         check(lib().gf_sweeps(self._h, ALGOS[algo], n, param, seed, rng_counter), "gf_sweeps")
 
