@@ -1124,7 +1124,8 @@ __device__ __forceinline__ bool grid_barrier(ChunkSync *sy, unsigned int arrival
             atomicAdd(&sy->gen, 1u);
         } else {
             const unsigned long long t0 = global_ns();
-            while (*vgen == g) {
+            for (unsigned int spin = 0; *vgen == g; spin++) {
+                if ((spin & 31u) != 31u) continue;  // poll the generation; the error word and the clock less often
                 if (*verr) {
                     ok = 0;
                     break;
@@ -1134,7 +1135,6 @@ __device__ __forceinline__ bool grid_barrier(ChunkSync *sy, unsigned int arrival
                     ok = 0;
                     break;
                 }
-                __nanosleep(100);
             }
         }
         __threadfence();

@@ -193,28 +193,29 @@ def test_landau_app_fix_with_sa_matches_oracle_driver(cuda):
 
 def test_mag_app_fix_matches_oracle_driver(cuda):
     """The MAG app's whole schedule in FP64 -- random trafo, the SA do-while (5 heat-bath sweeps, each
-    with a microcanonical sweep, per temperature, the step slowed 15x in [0.7, 0.88]), SR until
+    with a microcanonical sweep, per temperature, the step slowed 15x in its window), SR until
     theta < 1e-6, OR to theta < 1e-12, reprojections -- through gf_fix and through the oracle's
     restatement of apps/MAGaugeFixingSU3_4D.cu:222-333 on the same input and Philox key/counters:
     the same sweep count in every phase, the same functional, and the same field up to the
-    diagonal U(1) x U(1) transformations that leave the MAG functional unchanged.  (Those are flat
-    directions: rounding differences of the two summation orders, amplified by a hundred heat-bath
-    sweeps, move the two runs apart along them, so the field is compared through |U_ij|.)"""
+    diagonal U(1) x U(1) transformations that leave the MAG functional unchanged (compared through
+    |U_ij|).  The anneal is short and cold: a hot heat bath amplifies the rounding differences of
+    the two summation orders until the runs end at different maxima of equal functional."""
     from su3_ma_gauge_gpu_b200.engine import GaugeFixer, Schedule
 
     size = (4, 4, 4, 8)
     U, _ = S.smooth_config(size, 0.3, 91)
     prec = float(np.float32(1e-12))
-    sch = Schedule.mag_app(random_trafo=1, sa_steps=8, sa_min=0.01, sa_max=1.4, micro_updates=1, or_max_iter=4000,
-                           precision=prec, check_precision=10, reproject=20, seed=3, rng_counter=5)
+    sch = Schedule.mag_app(random_trafo=1, sa_steps=3, sa_min=0.1, sa_max=0.5, sa_slow_lo=0.2, sa_slow_hi=0.3,
+                           micro_updates=1, or_max_iter=4000, precision=prec, check_precision=10, reproject=20,
+                           seed=3, rng_counter=5)
     with GaugeFixer([size], gauge="mag", mixed=False) as gf:
         gf.load(0, U)
         rep = gf.fix(sch)[0]
         out = np.zeros_like(U)
         gf.store(0, out)
     ref = U.copy()
-    osch = O.app_schedule(random_trafo=1, sa_steps=8, sa_min=0.01, sa_max=1.4, micro_updates=1, sa_mode=2,
-                          sa_repeat=5, sa_slow_lo=0.7, sa_slow_hi=0.88, sa_slow_factor=15.0, sr_max_iter=1000,
+    osch = O.app_schedule(random_trafo=1, sa_steps=3, sa_min=0.1, sa_max=0.5, micro_updates=1, sa_mode=2,
+                          sa_repeat=5, sa_slow_lo=0.2, sa_slow_hi=0.3, sa_slow_factor=15.0, sr_max_iter=1000,
                           sr_parameter=1.7, sr_stop_theta=1e-6, or_max_iter=4000, precision=prec, check_precision=10,
                           reproject=20, seed=3)
     r, _ = O.fix_app(ref, size, O.MAG, osch, counter=5)
