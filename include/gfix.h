@@ -81,6 +81,12 @@ int gf_sr_step(int gauge, int real, void *U, void *Udw, const int32_t size[4], i
 int gf_random_trafo(int gauge, int real, void *U, void *Udw, const int32_t size[4], int parity,
                     int seed, int rng_counter, void *stream);
 
+/* One parity pass of update rule `algo` (0 OR, 1 micro, 2 SA, 3 SR, 4 random) over the sites of
+ * timeslices [t_begin, t_end) only, 4D gauges: the slab pass of the reference's MPI driver split
+ * into boundary and interior (apps/MultiGPU_MPI/MultiGPU_MPI_Communicator.hxx:351-430), so the
+ * interior runs while the boundary links are exchanged.  Philox as gf_sa_step. */
+int gf_step_slices(int gauge, int real, int algo, void *U, const int32_t size[4], int parity, float param,
+                   int seed, int rng_counter, int t_begin, int t_end, void *stream);
 /* *KernelsSU3::generateGaugeQualityPerSite (LandauKernelsSU3.hxx:71-74): per-site functional
  * and theta terms into device arrays of V doubles (either may be NULL). */
 int gf_quality_per_site(int gauge, int real, const void *U, const int32_t size[4], double *dGff,

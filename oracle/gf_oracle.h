@@ -56,6 +56,12 @@ void orc_step_f64(double *Uup, double *Udw, const int32_t size[4], int gauge, in
 void orc_step_f32(float *Uup, float *Udw, const int32_t size[4], int gauge, int algo, int parity,
                   float param, uint32_t seed, uint32_t counter, int nthreads);
 
+/* The same pass over the half-lattice sites h in [h_lo, h_hi) only (a timeslice range of a t-slab). */
+void orc_step_range_f64(double *Uup, double *Udw, const int32_t size[4], int gauge, int algo, int parity,
+                        float param, uint32_t seed, uint32_t counter, int64_t h_lo, int64_t h_hi, int nthreads);
+void orc_step_range_f32(float *Uup, float *Udw, const int32_t size[4], int gauge, int algo, int parity,
+                        float param, uint32_t seed, uint32_t counter, int64_t h_lo, int64_t h_hi, int nthreads);
+
 /* Gauge quality (a18, a19): per-site arrays (optional, may be NULL) and the normalised
  * functional and theta as GaugeFixingStats::generateGaugeQuality (GaugeFixingStats.hxx:186-232)
  * returns them.  stop_max = 0 -> AVERAGE, 1 -> MAX.  For COULOMB pass the slice array with

@@ -377,15 +377,15 @@ static void FN(subgroup)(MAT M[8], int i, int j, int gauge, int algo, float para
 
 /* One parity pass (the apply() of LandauKernelsSU3.hxx:216-256, CoulombKernelsSU3.hxx:208-250,
  * MAGKernelsSU3.hxx:248-293, U1xU1KernelsSU3.hxx:216-256), serial over sites. */
-void FN(orc_step)(REAL *Uup, REAL *Udw, const int32_t size[4], int gauge, int algo, int parity,
-                  float param, uint32_t seed, uint32_t counter, int nthreads)
+void FN(orc_step_range)(REAL *Uup, REAL *Udw, const int32_t size[4], int gauge, int algo, int parity,
+                        float param, uint32_t seed, uint32_t counter, int64_t h_lo, int64_t h_hi, int nthreads)
 {
     const int64_t V = (int64_t)size[0] * size[1] * size[2] * size[3];
     const int64_t Vh = V / 2;
     if (nthreads < 1) nthreads = 1;
     if (Udw == 0) Udw = Uup;
 #pragma omp parallel for num_threads(nthreads) schedule(static)
-    for (int64_t h = 0; h < Vh; h++) {
+    for (int64_t h = h_lo; h < h_hi; h++) {
         const int64_t s = h + (parity ? Vh : 0);
         MAT M[8];
         int64_t site[8];
@@ -415,6 +415,13 @@ void FN(orc_step)(REAL *Uup, REAL *Udw, const int32_t size[4], int gauge, int al
         FN(subgroup)(M, 0, 1, gauge, algo, param, &rng);
         for (int k = 0; k < 8; k++) FN(store12)(arr[k], V, site[k], k & 3, &M[k]);
     }
+}
+
+void FN(orc_step)(REAL *Uup, REAL *Udw, const int32_t size[4], int gauge, int algo, int parity,
+                  float param, uint32_t seed, uint32_t counter, int nthreads)
+{
+    const int64_t Vh = (int64_t)size[0] * size[1] * size[2] * size[3] / 2;
+    FN(orc_step_range)(Uup, Udw, size, gauge, algo, parity, param, seed, counter, 0, Vh, nthreads);
 }
 
 /* ---- gauge quality ------------------------------------------------------------------------- */

@@ -81,6 +81,45 @@ __global__ void __launch_bounds__(128) k_parity_pass(F Fup, F Fdw, Geom g, int p
     parity_pass_warp<R, GAUGE, ALGO>(Fup, Fdw, g, warp, parity, p);
 }
 
+// One parity pass over the sites of timeslices [t_begin, t_end) only (4D gauges): in the
+// parity-split order those sites are the contiguous run h in [t_begin Vs/2, t_end Vs/2), so the
+// warps cover that run from its 8-aligned start and leave the sites outside it alone.  A t-slab
+// rank updates its interior slices with it while the boundary links are on their way.
+template <typename R, int GAUGE, int ALGO, class F>
+__global__ void __launch_bounds__(128) k_parity_pass_range(F f, Geom g, int parity, AlgoParams p, int64_t h_lo,
+                                                           int64_t h_hi)
+{
+    static_assert(GAUGE != COULOMB, "timeslice ranges are for the 4D gauges");
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31, mu = lane >> 3;
+    const int64_t h0 = (h_lo & ~(int64_t)7) + warp * 8;
+    if (h0 >= h_hi) return;  // warp-uniform
+    const int64_t h = h0 + (lane & 7);
+    const bool active = h >= h_lo && h < h_hi;  // the same for the 4 lanes of a site
+    int64_t s = 0, sd = 0;
+    Link<R> up, dn;
+    if (active) {
+        int32_t c[4];
+        site_coords(g, h, parity, c);
+        s = h + (parity ? g.Vh : 0);
+        sd = neighbour_down(g, c, mu);
+        load_link<R>(f, s, mu, up);
+        load_link<R>(f, sd, mu, dn);
+    } else {  // no coupling: the update leaves these (unstored) links alone
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) up.e[i][j] = dn.e[i][j] = cx<R>((R)0, (R)0);
+    }
+    Rng<R> rng;
+    if (ALGO == ALG_SA || ALGO == ALG_SR || ALGO == ALG_RANDOM) rng.init(ref_rng_tid(h), p.seed, p.counter);
+    site_update<GAUGE, ALGO>(up, dn, mu, p, rng);
+    if (active) {
+        store_link<R>(f, s, mu, up);
+        store_link<R>(f, sd, mu, dn);
+    }
+}
+
 // ---- gauge quality ---------------------------------------------------------------------------
 template <typename R, class F>
 __device__ __forceinline__ void load_link_f64(const F &f, int64_t s, int mu, Link<double> &L)

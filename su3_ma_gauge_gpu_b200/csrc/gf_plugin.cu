@@ -118,6 +118,32 @@ static int plugin_step(int gauge, int real, int algo, void *U, void *Udw, const 
     return dispatch_gauge_algo<RefStep>(gauge, algo, a);
 }
 
+struct RangeArgs {
+    StepArgs a;
+    int64_t h_lo, h_hi;
+};
+
+template <int GAUGE, int ALGO>
+struct RefStepRange {
+    template <typename R>
+    static int go(const RangeArgs &r)
+    {
+        if constexpr (GAUGE == COULOMB) {
+            set_error("timeslice ranges are for the 4D gauges");
+            return GF_ERR_INVALID;
+        } else {
+            RefField<R> fu{(R *)r.a.U, r.a.g.V};
+            const int64_t warps = (r.h_hi - (r.h_lo & ~(int64_t)7) + 7) / 8;
+            if (warps <= 0) return GF_OK;
+            const unsigned blocks = (unsigned)((warps * 32 + 127) / 128);
+            k_parity_pass_range<R, GAUGE, ALGO, RefField<R>><<<blocks, 128, 0, r.a.stream>>>(fu, r.a.g, r.a.parity, r.a.p,
+                                                                                          r.h_lo, r.h_hi);
+            return launch_status("parity pass over timeslices");
+        }
+    }
+    static int run(const RangeArgs &r) { return r.a.real == GF_FP64 ? go<double>(r) : go<float>(r); }
+};
+
 // ---- quality -----------------------------------------------------------------------------------
 struct QualityArgs {
     int real;
@@ -211,6 +237,37 @@ int gf_random_trafo(int gauge, int real, void *U, void *Udw, const int32_t size[
                     int rng_counter, void *stream)
 {
     return plugin_step(gauge, real, ALG_RANDOM, U, Udw, size, parity, 0.f, seed, rng_counter, stream);
+}
+
+int gf_step_slices(int gauge, int real, int algo, void *U, const int32_t size[4], int parity, float param, int seed,
+                   int rng_counter, int t_begin, int t_end, void *stream)
+{
+    clear_error();
+    if (!valid_gauge(gauge) || gauge == GF_COULOMB || !valid_real(real) || !U || (parity != 0 && parity != 1) ||
+        algo < ALG_OR || algo > ALG_RANDOM) {
+        set_error("invalid argument to gf_step_slices (4D gauges only)");
+        return GF_ERR_INVALID;
+    }
+    RangeArgs r;
+    int st = make_geom(size, gauge, false, r.a.g);
+    if (st) return st;
+    if (t_begin < 0 || t_end > size[0] || t_begin > t_end) {
+        set_error("timeslice range [%d, %d) is not inside [0, %d)", t_begin, t_end, size[0]);
+        return GF_ERR_INVALID;
+    }
+    const int64_t half_slice = r.a.g.V / size[0] / 2;
+    r.h_lo = t_begin * half_slice;
+    r.h_hi = t_end * half_slice;
+    r.a.real = real;
+    r.a.U = U;
+    r.a.Udw = U;
+    r.a.parity = parity;
+    r.a.p.param = param;
+    r.a.p.seed = (uint32_t)seed;
+    r.a.p.counter = (uint32_t)rng_counter;
+    r.a.p.counter_stride = 0;
+    r.a.stream = (cudaStream_t)stream;
+    return dispatch_gauge_algo<RefStepRange>(gauge, algo, r);
 }
 
 double gf_quality_prefactor_gff(int gauge) { return prefactor_gff(gauge); }

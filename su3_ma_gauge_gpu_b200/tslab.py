@@ -18,10 +18,22 @@ GPUs, gloo on CPU) around the library's own parity pass, unchanged:
   write only halo links and the wrapped parity-(1-p) temporal links of the last owned slice --
   exactly the links the returned message overwrites.  Nothing owned is left corrupted.
 
-The message is tiny next to the pass (Vs/2 x 12 reals per boundary, about 2.6 MB for 48^3 in
-FP32), so it is sent with plain send/recv; the functional and theta are summed with all_reduce.
-Only deterministic updates (overrelaxation, microcanonical) give the single-lattice result bit
-for bit: the heat-bath draws its Philox numbers by local site index.
+In the GpuPattern layout the message is a plain block of the field: the temporal links of slice t
+and parity q are the contiguous run h in [t Vs/2, (t+1) Vs/2) of the parity-q half of each of the
+12 planes of rows 0 and 1 -- a (12, Vs/2) slice with row stride V.  So messages are packed and
+unpacked by one strided copy each, never by index lists.
+
+SlabExchange runs a pass with the exchange overlapped, as the reference splits its pass
+(MultiGPU_MPI_Communicator.hxx:351-430): the forward message is posted first, the interior slices
+(which read no halo) are updated while it travels, then the last owned slice (once the previous
+pass's returned links are in), then the first owned slice from the halo, and the return message
+is posted without waiting -- the next pass waits for it only before it updates the last slice.
+The halo sites themselves are never updated.  With NCCL the waits are stream dependencies, so the
+host never blocks inside a sweep.
+
+The functional and theta are summed with all_reduce.  Only deterministic updates
+(overrelaxation, microcanonical) give the single-lattice result bit for bit: the heat-bath draws
+its Philox numbers by local site index.
 """
 from __future__ import annotations
 
@@ -57,14 +69,6 @@ class TSlab:
         self._xyz = (x, y, z)
         V = self.V
         ls = self.local_size
-        # reals 0..11 (rows 0, 1) of U_t at local slice `t` for the sites of parity `q`, in (x, y, z) order
-        def t_rows(t, q):
-            sel = ((t + x + y + z) % 2) == q
-            s = _site_index(ls, np.full(sel.sum(), t), x[sel], y[sel], z[sel])
-            return (s[:, None] + V * np.arange(12)[None, :]).reshape(-1)  # mu = 0: offset 18*0*V
-        # before / after the pass of parity p the parity-(1-p) links move between slabs
-        self._halo = {p: t_rows(1, 1 - p) for p in (0, 1)}
-        self._last = {p: t_rows(self.T + 1, 1 - p) for p in (0, 1)}
         # owned sites (slices 2 .. T+1) in local parity-split order, and their global indices
         tl = np.repeat(np.arange(2, self.T + 2), self.Vs)
         xx, yy, zz = (np.tile(a, self.T) for a in (x, y, z))
@@ -113,31 +117,28 @@ class TSlab:
                                                                                          device=dev)]
 
     # ---- the exchange ---------------------------------------------------------------------------
-    def _idx(self, which, p, U):
-        idx = which[p]
-        if isinstance(U, np.ndarray):
-            return idx
-        import torch
-
-        key = (id(which), p, str(U.device))
-        cache = self.__dict__.setdefault("_tidx", {})
-        if key not in cache:
-            cache[key] = torch.as_tensor(idx, device=U.device)
-        return cache[key]
+    def rows_view(self, U, t, q):
+        """Rows 0, 1 (the 12 stored reals) of the temporal links of local slice t, sites of parity q:
+        a (12, Vs/2) view of the GpuPattern array U (numpy array or tensor; no copy)."""
+        half = self.Vs // 2
+        s0 = t * half + q * (self.V // 2)
+        return U.reshape(72, self.V)[:12, s0:s0 + half]
 
     def boundary_out(self, U, p):
-        """Before the pass of parity p: what goes to rank r+1 (its halo)."""
-        return U[self._idx(self._last, p, U)]
+        """Before the pass of parity p: what goes to rank r+1 (its halo), a contiguous copy."""
+        v = self.rows_view(U, self.T + 1, 1 - p)
+        return v.copy() if isinstance(v, np.ndarray) else v.clone()
 
     def halo_in(self, U, p, msg):
-        U[self._idx(self._halo, p, U)] = msg
+        self.rows_view(U, 1, 1 - p)[...] = msg
 
     def halo_out(self, U, p):
         """After the pass of parity p: the updated halo links that go back to rank r-1."""
-        return U[self._idx(self._halo, p, U)]
+        v = self.rows_view(U, 1, 1 - p)
+        return v.copy() if isinstance(v, np.ndarray) else v.clone()
 
     def boundary_in(self, U, p, msg):
-        U[self._idx(self._last, p, U)] = msg
+        self.rows_view(U, self.T + 1, 1 - p)[...] = msg
 
     def owned_sum(self, per_site):
         """Sum of a per-site array (local parity-split order) over the owned sites."""
@@ -245,6 +246,124 @@ def emulate_parity_pass(slabs, Us, parity: int, run_pass):
     backs = [slabs[r].halo_out(Us[r], parity) for r in range(world)]
     for r in range(world):
         slabs[r].boundary_in(Us[r], parity, backs[(r + 1) % world])
+
+
+class SlabExchange:
+    """Parity passes of one slab with the boundary exchange overlapped (see the module docstring).
+
+    run_slices(U, local_size, parity, t_begin, t_end) updates the sites of local slices
+    [t_begin, t_end) (gpu_or_slices for the library's pass).  Buffers are allocated once; call
+    finish() after the last pass (before reading the last owned slice or the functional)."""
+
+    def __init__(self, slab: TSlab, U, group=None):
+        self.slab, self.group = slab, group
+        self.host = isinstance(U, np.ndarray)
+        shape = (12, slab.Vs // 2)
+        if self.host:
+            self.buf = {k: np.empty(shape, dtype=U.dtype) for k in ("fs", "fr", "bs", "br")}
+        else:
+            import torch
+
+            self.buf = {k: torch.empty(shape, dtype=U.dtype, device=U.device) for k in ("fs", "fr", "bs", "br")}
+        self.pending = None  # (works of the return exchange, parity of its links)
+
+    def _post(self, send, to, recv, frm):
+        """send -> rank `to`, recv <- rank `frm`; returns the works (a local copy for one rank)."""
+        if self.slab.world == 1:
+            recv[...] = send
+            return []
+        import torch
+        import torch.distributed as dist
+
+        s = torch.from_numpy(send) if self.host else send
+        r = torch.from_numpy(recv) if self.host else recv
+        return dist.batch_isend_irecv([dist.P2POp(dist.isend, s, to, self.group),
+                                       dist.P2POp(dist.irecv, r, frm, self.group)])
+
+    @staticmethod
+    def _wait(works):
+        for w in works:
+            w.wait()  # NCCL: the current stream waits; gloo: the host waits
+
+    def _finish_return(self, U):
+        if self.pending is not None:
+            works, q = self.pending
+            self._wait(works)
+            self.slab.rows_view(U, self.slab.T + 1, q)[...] = self.buf["br"]
+            self.pending = None
+
+    def parity_pass(self, U, p, run_slices):
+        sl = self.slab
+        T, ls = sl.T, sl.local_size
+        nxt, prv = (sl.rank + 1) % sl.world, (sl.rank - 1) % sl.world
+        b = self.buf
+        b["fs"][...] = sl.rows_view(U, T + 1, 1 - p)
+        fwd = self._post(b["fs"], nxt, b["fr"], prv)
+        run_slices(U, ls, p, 3, T + 1)        # interior: reads no halo and no returned link
+        self._finish_return(U)                # the previous pass's links, updated by rank r+1
+        run_slices(U, ls, p, T + 1, T + 2)    # last owned slice
+        self._wait(fwd)
+        sl.rows_view(U, 1, 1 - p)[...] = b["fr"]
+        run_slices(U, ls, p, 2, 3)            # first owned slice, from the halo
+        b["bs"][...] = sl.rows_view(U, 1, 1 - p)
+        self.pending = (self._post(b["bs"], prv, b["br"], nxt), 1 - p)
+
+    def finish(self, U):
+        self._finish_return(U)
+
+
+def emulate_overlapped_pass(slabs, Us, parity: int, run_slices, pending):
+    """SlabExchange.parity_pass for all ranks of one process (one GPU or CPU), the ranks' steps
+    interleaved in the order the messages allow: every message is a copy and no rank waits on
+    another inside a kernel.  `pending` carries the return messages between passes (start with {};
+    call emulate_finish at the end)."""
+    world = len(slabs)
+    p = parity
+    outs = [slabs[r].boundary_out(Us[r], p) for r in range(world)]
+    for r in range(world):
+        run_slices(Us[r], slabs[r].local_size, p, 3, slabs[r].T + 1)
+    emulate_finish(slabs, Us, pending)
+    for r in range(world):
+        run_slices(Us[r], slabs[r].local_size, p, slabs[r].T + 1, slabs[r].T + 2)
+    for r in range(world):
+        slabs[r].halo_in(Us[r], p, outs[(r - 1) % world])
+        run_slices(Us[r], slabs[r].local_size, p, 2, 3)
+    backs = [slabs[r].halo_out(Us[r], p) for r in range(world)]
+    pending.update({r: (backs[(r + 1) % world], p) for r in range(world)})
+
+
+def emulate_finish(slabs, Us, pending):
+    for r, (msg, p) in list(pending.items()):
+        slabs[r].boundary_in(Us[r], p, msg)
+    pending.clear()
+
+
+def gpu_or_slices(omega: float = 1.7, gauge: str = "landau", precision: str = "double"):
+    """run_slices for SlabExchange: the library's OR pass over a range of timeslices
+    (gf_step_slices) on the local lattice, CUDA tensors."""
+    import ctypes
+
+    from . import _lib
+
+    g = {"landau": _lib.GF_LANDAU, "mag": _lib.GF_MAG, "u1xu1": _lib.GF_U1XU1}.get(gauge)
+    if g is None:
+        raise ValueError("t-slabs are for the 4D gauges (landau, mag, u1xu1)")
+    real = _lib.GF_FP64 if precision in ("double", "fp64") else _lib.GF_FP32
+    sizes = {}
+
+    def run(U, local_size, parity, t_begin, t_end):
+        if t_end <= t_begin:
+            return
+        s = sizes.get(local_size)
+        if s is None:
+            s = sizes[local_size] = _lib.size_arg(local_size)
+        import torch
+
+        stream = torch.cuda.current_stream().cuda_stream
+        _lib.check(_lib.lib().gf_step_slices(g, real, 0, ctypes.c_void_p(U.data_ptr()), s, parity, ctypes.c_float(omega),
+                                             0, 0, t_begin, t_end, ctypes.c_void_p(stream)), "gf_step_slices")
+
+    return run
 
 
 def gpu_or_pass(omega: float = 1.7, gauge: str = "landau", precision: str = "double"):

@@ -11,14 +11,19 @@ import pytest
 
 import _oracle as O
 from su3_ma_gauge_gpu_b200 import synthetic as S
-from su3_ma_gauge_gpu_b200.tslab import (TSlab, emulate_parity_pass, emulate_refresh_halo, gpu_or_pass, parity_pass,
-                                        quality)
+from su3_ma_gauge_gpu_b200.tslab import (SlabExchange, TSlab, emulate_finish, emulate_overlapped_pass,
+                                        emulate_parity_pass, emulate_refresh_halo, gpu_or_pass, gpu_or_slices,
+                                        parity_pass, quality)
 
 SIZE = (8, 4, 6, 4)
 
 
 def _oracle_pass(U, size, parity):
     O.step(U, size, O.LANDAU, O.OR, parity, 1.7, nthreads=2)
+
+
+def _oracle_slices(U, size, parity, t_begin, t_end):
+    O.step_slices(U, size, O.LANDAU, O.OR, parity, t_begin, t_end, 1.7, nthreads=2)
 
 
 def _reference(U, nsweeps):
@@ -83,6 +88,28 @@ def test_emulated_slabs_match_single_lattice(world):
     assert ts == pytest.approx(float(a.sum()), rel=1e-11)
 
 
+@pytest.mark.parametrize("world", [1, 2, 4])
+def test_emulated_overlapped_slabs_match_single_lattice(world):
+    """The overlapped pass -- interior slices while the forward message travels, then the last
+    owned slice, then the first from the halo, the return message waited for only by the next
+    pass -- gives the single-lattice sweep bit for bit, without ever updating the halo sites."""
+    U, _ = S.smooth_config(SIZE, 0.3, 36)
+    slabs = [TSlab(SIZE, r, world) for r in range(world)]
+    Us = [s.scatter(U) for s in slabs]
+    halos = [L.reshape(72, -1)[:, :2 * s.Vs // 2].copy() for s, L in zip(slabs, Us)]  # parity-0 halo sites
+    pending = {}
+    for _ in range(3):
+        for p in (0, 1):
+            emulate_overlapped_pass(slabs, Us, p, _oracle_slices, pending)
+    emulate_finish(slabs, Us, pending)
+    out = np.zeros_like(U)
+    for s, L in zip(slabs, Us):
+        s.gather_into(L, out)
+    assert np.array_equal(out, _reference(U, 3))
+    for s, L, h0 in zip(slabs, Us, halos):  # halo slice 0's parity-0 sites: never updated
+        assert np.array_equal(L.reshape(72, -1)[12:, :s.Vs // 2], h0[12:, :s.Vs // 2])
+
+
 def _free_port():
     s = socket.socket()
     s.bind(("127.0.0.1", 0))
@@ -91,7 +118,7 @@ def _free_port():
     return p
 
 
-def _rank(rank, world, port, U, q):
+def _rank(rank, world, port, U, q, overlapped=False):
     import datetime
 
     import torch.distributed as dist
@@ -101,9 +128,15 @@ def _rank(rank, world, port, U, q):
     try:
         slab = TSlab(SIZE, rank, world)
         L = slab.scatter(U)
+        ex = SlabExchange(slab, L) if overlapped else None
         for _ in range(2):
             for p in (0, 1):
-                parity_pass(slab, L, p, _oracle_pass)
+                if overlapped:
+                    ex.parity_pass(L, p, _oracle_slices)
+                else:
+                    parity_pass(slab, L, p, _oracle_pass)
+        if overlapped:
+            ex.finish(L)
         sums = quality(slab, L, lambda A, size: O.quality(A, size, O.LANDAU, per_site=True)[2:])
         out = np.zeros_like(U)
         slab.gather_into(L, out)
@@ -112,14 +145,15 @@ def _rank(rank, world, port, U, q):
         dist.destroy_process_group()
 
 
-def test_gloo_two_ranks_match_single_lattice():
+@pytest.mark.parametrize("overlapped", [False, True], ids=["whole-pass", "overlapped"])
+def test_gloo_two_ranks_match_single_lattice(overlapped):
     import torch.multiprocessing as mp
 
     U, _ = S.smooth_config(SIZE, 0.3, 32)
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_rank, args=(r, 2, port, U, q)) for r in range(2)]
+    procs = [ctx.Process(target=_rank, args=(r, 2, port, U, q, overlapped)) for r in range(2)]
     for p in procs:
         p.start()
     got = [q.get(timeout=180) for _ in procs]
@@ -163,3 +197,38 @@ def test_gpu_slabs_match_plugin_pass(cuda, world):
     for s, L in zip(slabs, Us):
         s.gather_into(L, out)
     assert torch.equal(out, dU)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("world", [1, 2, 4])
+def test_gpu_overlapped_slabs_match_plugin_pass(cuda, world):
+    """The overlapped slab pass with the library's timeslice-range pass (gf_step_slices), ranks
+    emulated on one GPU in the order the messages allow, against the whole-lattice plugin pass;
+    and the range pass over slices [0, a) + [a, Nt) equals the whole pass."""
+    torch = cuda
+    from su3_ma_gauge_gpu_b200 import LandauKernelsSU3
+
+    U, _ = S.smooth_config(SIZE, 0.3, 37)
+    dU = torch.from_numpy(U).cuda()
+    k = LandauKernelsSU3(SIZE, "double")
+    for _ in range(3):
+        for p in (0, 1):
+            k.orStep(0, 0, dU, None, p, 1.7)
+    run = gpu_or_slices(1.7)
+    slabs = [TSlab(SIZE, r, world) for r in range(world)]
+    Us = [s.scatter(torch.from_numpy(U).cuda(), xp=torch) for s in slabs]
+    pending = {}
+    for _ in range(3):
+        for p in (0, 1):
+            emulate_overlapped_pass(slabs, Us, p, run, pending)
+    emulate_finish(slabs, Us, pending)
+    out = torch.zeros_like(dU)
+    for s, L in zip(slabs, Us):
+        s.gather_into(L, out)
+    assert torch.equal(out, dU)
+    A = torch.from_numpy(U).cuda()
+    B = torch.from_numpy(U).cuda()
+    k.orStep(0, 0, A, None, 1, 1.7)
+    run(B, SIZE, 1, 0, 3)
+    run(B, SIZE, 1, 3, SIZE[0])
+    assert torch.equal(A, B)
