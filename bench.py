@@ -268,27 +268,33 @@ def reference_gpu_leg(dU_in, gpu_id, fixes) -> dict | None:
 
 def run_profile_target(nsweeps: int, mode: str = "fast"):
     """A short, fixed launch sequence of the hot kernels for ncu (see profiles/): the 32^4 input,
-    `nsweeps` OR sweeps per launch shape in FP32, then the same in FP64.
-    mode "fast": FP32 storage; shapes direct, pipelined (4 warps per block) -- 8 * nsweeps
-    parity-pass launches.  mode "refine": FP64 master + FP32 working copy with W; FP32 shapes
-    direct, 64-register, register prefetch, thread per site (plain, pipelined), then FP64 direct,
-    pipelined (4), register prefetch -- 16 * nsweeps parity-pass launches."""
+    `nsweeps` OR sweeps per launch shape in FP32, then the same in FP64 (shape = (variant, walk
+    order), gf_set_pass_shape / gf_set_pass_order).
+    mode "fast": FP32 storage; FP32 shapes direct, pipelined, two lanes per site (direct, register
+    prefetch, register prefetch with alternating walk); FP64 direct, pipelined (alternating walk).
+    mode "refine": FP64 master + FP32 working copy with W; FP32 shapes direct, 64-register, register
+    prefetch, thread per site (plain, pipelined), two lanes per site (direct, register prefetch, with
+    alternating walk); then FP64 direct, pipelined (4 warps; with alternating walk), register prefetch."""
     import torch
 
     from su3_ma_gauge_gpu_b200 import synthetic as S
     from su3_ma_gauge_gpu_b200.engine import GaugeFixer
 
-    U, _ = S.smooth_config(SIZE, EPS, 1234, device="cuda")
+    dU, _ = S.smooth_config(SIZE, EPS, 1234, device="cuda", as_tensor=True)
     torch.cuda.empty_cache()  # keep the device footprint of the profiled launches small
-    dU = torch.from_numpy(U).cuda()
-    shapes = {"fp32": (0, 1), "fp64": (0, 1)} if mode == "fast" else {"fp32": (0, 2, 3, 4, 5), "fp64": (0, 1, 3)}
+    if mode == "fast":
+        shapes = {"fp32": [(0, 0), (1, 0), (6, 0), (7, 0), (7, 1)], "fp64": [(0, 0), (1, 0), (1, 1)]}
+    else:
+        shapes = {"fp32": [(0, 0), (2, 0), (3, 0), (4, 0), (5, 0), (6, 0), (7, 0), (7, 1)],
+                  "fp64": [(0, 0), (1, 0), (1, 1), (3, 0)]}
     with GaugeFixer([SIZE], mixed=True if mode == "fast" else "refine") as gf:
         gf.load(0, dU)
         for real in ("fp32", "fp64"):
             if real == "fp64":
                 gf.to_fp64()
-            for variant in shapes[real]:
+            for variant, alt in shapes[real]:
                 gf.set_pass_shape(real, variant, 4)
+                gf.set_pass_order(real, bool(alt))
                 gf.sweeps("or", nsweeps, 1.7)
         g, a = gf.quality()
         gf.store(0, dU)
