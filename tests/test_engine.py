@@ -483,7 +483,8 @@ def test_autotune_picks_a_shape(cuda):
         before = np.zeros_like(U)
         gf.store(0, before)
         c32, c64 = gf.autotune()
-        assert c32 in (0, 64, 100, 32, 33, 16, 116, 2, 4, 8) and c64 in (0, 100, 16, 2, 4, 8)
+        # codes + 1000: the same shape with the alternating walk (gf_set_pass_order)
+        assert c32 % 1000 in (0, 64, 100, 32, 33, 16, 116, 2, 4, 8) and c64 % 1000 in (0, 100, 16, 2, 4, 8)
         after = np.zeros_like(U)
         gf.store(0, after)
         assert np.array_equal(before, after)  # tuning ran on a scratch copy
