@@ -48,6 +48,8 @@ BYTES_PER_SITE_UPDATE = {"fp32": 768, "fp64": 1536, "fp32_refine": 768 + 96}
 
 def pass_kernel_name(code: int, real: str, refine: bool) -> str:
     """The OR-pass kernel an autotuner choice stands for (gf_autotune's output codes)."""
+    if code >= 10000:
+        return pass_kernel_name(code - 10000, real, refine) + ", registers capped"
     if code >= 1000:
         return pass_kernel_name(code - 1000, real, refine) + ", odd-parity passes walked backwards"
     r = "float" if real == "fp32" else "double"
@@ -67,6 +69,16 @@ def pass_kernel_name(code: int, real: str, refine: bool) -> str:
     if code in (2, 4, 8):
         return f"k_batched_pass_staged<{r}, LANDAU, OR, {code} warps>"
     return f"k_batched_pass<{r}, LANDAU, OR{w}>"
+
+
+def apply_pass_code(gf, real: str, code: int) -> None:
+    """Set the OR-pass launch shape an autotuner code stands for (gf_autotune's output codes)."""
+    capped, code = code >= 10000, code % 10000
+    alternate, code = code >= 1000, code % 1000
+    variant, warps = {0: (0, 4), 64: (2, 4), 100: (3, 4), 32: (4, 4), 33: (5, 4), 16: (6, 4), 116: (7, 4),
+                      2: (1, 2), 4: (1, 4), 8: (1, 8)}[code]
+    gf.set_pass_shape(real, variant, warps)
+    gf.set_pass_order(real, alternate, capped)
 
 
 def env_rank():
@@ -304,29 +316,38 @@ def run_profile_target(nsweeps: int, mode: str = "fast"):
 
 def run_launch_list(args):
     """One step of the headline workload (import + gf_fix + export of the 32^4 field, the bench's
-    mixed mode and schedule) for a profiler's launch list: no warm-up, no clock sampling, and the
-    check chunks launched directly instead of replayed from CUDA graphs (the same kernels in the
-    same order).  Prints how many of the library's launches came before the step (autotuning)."""
+    mixed mode and schedule) for a profiler's launch list: no warm-up, no clock sampling, the check
+    chunks launched directly instead of replayed from CUDA graphs (the same kernels in the same
+    order), the step inside the NVTX range "headline_step" (ncu --nvtx --nvtx-include
+    "headline_step/").  --pass-fp32 / --pass-fp64 fix the launch shapes by autotuner code (a
+    profiler distorts the autotuner's timings); without them the autotuner picks."""
     import torch
 
     from su3_ma_gauge_gpu_b200 import synthetic as S
     from su3_ma_gauge_gpu_b200.engine import GaugeFixer, Schedule
 
-    U, _ = S.smooth_config(SIZE, EPS, 1234, device="cuda")
+    dU, _ = S.smooth_config(SIZE, EPS, 1234, device="cuda", as_tensor=True)
     torch.cuda.empty_cache()
-    dU = torch.from_numpy(U).cuda()
     out = torch.empty_like(dU)
     sched = Schedule(or_max_iter=20000, precision=1e-12, switch_theta=args.switch_theta, check_precision=args.check,
-                     fold=args.fold, reproject=100, micro_updates=0, use_graphs=0)
+                     fold=args.fold, reproject=100, micro_updates=0, use_graphs=0, autotune=0)
     with GaugeFixer([SIZE], mixed="refine" if args.mixed == "refine" else True) as gf:
         gf.load(0, dU)
-        tuned = gf.autotune()
+        if args.pass_fp32 is not None and args.pass_fp64 is not None:
+            apply_pass_code(gf, "fp32", args.pass_fp32)
+            apply_pass_code(gf, "fp64", args.pass_fp64)
+            tuned = (args.pass_fp32, args.pass_fp64)
+        else:
+            tuned = gf.autotune()
         before = gf.kernel_launches()
         gf.load(0, dU)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_push("headline_step")
         rep = gf.fix(sched)[0]
         gf.store(0, out)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
         step = gf.kernel_launches() - before
-    torch.cuda.synchronize()
     print(json.dumps({"launch_list": "ok", "launches_before_step": before, "launches_in_step": step,
                       "launch_shape": tuned, "or_sweeps": rep.or_sweeps, "fp64_sweeps": rep.or_sweeps_fp64,
                       "theta": rep.theta}))
@@ -592,6 +613,8 @@ def main():
                     help="comma-separated configurations to run after the headline on a single GPU and report as "
                          "extra keys (plain8, coulomb48x16, gribov64, mag48), 'all' or 'none'")
     ap.add_argument("--profile-mode", default="fast", choices=["fast", "refine"])
+    ap.add_argument("--pass-fp32", type=int, default=None, help="launch-list mode: FP32 pass shape (autotuner code)")
+    ap.add_argument("--pass-fp64", type=int, default=None, help="launch-list mode: FP64 pass shape (autotuner code)")
     ap.add_argument("--launch-list", action="store_true",
                     help="one headline step without graphs, warm-up or clock sampling, for ncu's launch list")
     ap.add_argument("--profile", type=int, default=0, metavar="N",
@@ -758,19 +781,26 @@ def main():
     Vh = V // 2
     n64 = rep.or_sweeps_fp64
     n32 = sweeps - n64
-    b32 = BYTES_PER_SITE_UPDATE["fp32_refine" if args.mixed == "refine" else "fp32"]
+    # algorithmic bytes (8 links x 12 reals, read and written) -- the roofline's numerator; refine mode's
+    # FP32 pass also moves the two tracked columns of W - 1 (reported as gbs_moved)
+    b32 = BYTES_PER_SITE_UPDATE["fp32"]
+    m32 = BYTES_PER_SITE_UPDATE["fp32_refine" if args.mixed == "refine" else "fp32"]
     kern = {"fp32": {"ms_per_launch": t32, "gbs": Vh * b32 / (t32 * 1e-3) / 1e9, "launches_per_step": 2 * n32,
-                     "bytes_per_site_update": b32}}
+                     "bytes_per_site_update": b32, "bytes_moved_per_site_update": m32,
+                     "gbs_moved": Vh * m32 / (t32 * 1e-3) / 1e9}}
     if t64 is not None:
         kern["fp64"] = {"ms_per_launch": t64, "gbs": Vh * BYTES_PER_SITE_UPDATE["fp64"] / (t64 * 1e-3) / 1e9,
                         "launches_per_step": 2 * n64, "bytes_per_site_update": BYTES_PER_SITE_UPDATE["fp64"]}
     dom = max(kern, key=lambda k: kern[k]["ms_per_launch"] * kern[k]["launches_per_step"])
+    # dram bytes of one launch of the chosen kernel, from the ncu summaries (profiles/), keyed by mode and
+    # autotuner code; null when that kernel has not been captured
     traffic = None
     tfile = ROOT / "profiles" / "or_pass_traffic.json"
     if tfile.exists():
         try:
             tkey = "fp32_refine" if dom == "fp32" and args.mixed == "refine" else dom
-            traffic = json.loads(tfile.read_text()).get(tkey)
+            code = str(tuned[0 if dom == "fp32" else 1])
+            traffic = json.loads(tfile.read_text()).get(tkey, {}).get(code)
         except Exception:
             traffic = None
     roofline = {"bound": "hbm", "achieved": kern[dom]["gbs"], "peak": peak, "unit": "GB/s",

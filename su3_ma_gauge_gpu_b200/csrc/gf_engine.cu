@@ -102,6 +102,7 @@ struct gf_ctx {
     struct PassShape {
         int variant = 0, warps = 4, blocks_per_sm = 0;
         int alternate = 0;  // persistent variants (1, 3, 7): walk the tiles backwards on odd parities
+        int capped = 0;     // variants 1 (4 warps per block) and 7: registers capped for more resident warps
     } shape[2];
     int tuned[2] = {0, 0};
     // the lattices the caller passed: first instance and number of instances (Coulomb contexts
@@ -149,11 +150,11 @@ struct PassArgs {
     int reverse;  // persistent passes: walk the tiles backwards
 };
 
-template <typename R, int GAUGE, int ALGO, int WARPS>
+template <typename R, int GAUGE, int ALGO, int WARPS, int MINB = 1>
 int launch_staged(const gf_ctx *c, const EngineDev &e, const PassArgs &a, int blocks_per_sm)
 {
     const size_t smem = staged_smem_bytes<R>(WARPS);
-    auto kern = k_batched_pass_staged<R, GAUGE, ALGO, WARPS>;
+    auto kern = k_batched_pass_staged<R, GAUGE, ALGO, WARPS, MINB>;
     static bool smem_opt_in = false;  // above 48 KB the dynamic shared memory must be opted in
     if (!smem_opt_in) {
         int st = cuda_status(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
@@ -214,10 +215,10 @@ int launch_site_staged(const gf_ctx *c, const EngineDev &e, const PassArgs &a, i
     return launch_status("batched parity pass (thread per site, pipelined)");
 }
 
-template <typename R, int GAUGE, int ALGO, bool SITE_W>
+template <typename R, int GAUGE, int ALGO, bool SITE_W, int MINB = 1>
 int launch_pair_rp(const gf_ctx *c, const EngineDev &e, const PassArgs &a, int blocks_per_sm)
 {
-    auto kern = k_batched_pass_pair_rp<R, GAUGE, ALGO, SITE_W>;
+    auto kern = k_batched_pass_pair_rp<R, GAUGE, ALGO, SITE_W, MINB>;
     static int occ_cached = 0;  // resident blocks per SM of this instantiation
     int occ = blocks_per_sm;
     if (occ <= 0) {
@@ -242,6 +243,10 @@ int launch_pass(const gf_ctx *c, const EngineDev &e, const PassArgs &a, const gf
         // and the other rules when 7 is chosen)
         if constexpr (ALGO == ALG_OR && sizeof(R) == 4) {  // FP64 would spill at 255 registers
             if (sh.variant == 7) {
+                if (sh.capped) {  // 170 registers: 3 blocks of 4 warps per SM instead of 2
+                    if (c->site_w) return launch_pair_rp<R, GAUGE, ALGO, true, 3>(c, e, a, sh.blocks_per_sm);
+                    return launch_pair_rp<R, GAUGE, ALGO, false, 3>(c, e, a, sh.blocks_per_sm);
+                }
                 if (c->site_w) return launch_pair_rp<R, GAUGE, ALGO, true>(c, e, a, sh.blocks_per_sm);
                 return launch_pair_rp<R, GAUGE, ALGO, false>(c, e, a, sh.blocks_per_sm);
             }
@@ -293,7 +298,9 @@ int launch_pass(const gf_ctx *c, const EngineDev &e, const PassArgs &a, const gf
             switch (sh.warps) {
             case 2: return launch_staged<R, GAUGE, ALGO, 2>(c, e, a, sh.blocks_per_sm);
             case 8: return launch_staged<R, GAUGE, ALGO, 8>(c, e, a, sh.blocks_per_sm);
-            default: return launch_staged<R, GAUGE, ALGO, 4>(c, e, a, sh.blocks_per_sm);
+            default:
+                if (sh.capped) return launch_staged<R, GAUGE, ALGO, 4, 4>(c, e, a, sh.blocks_per_sm);  // 128 registers
+                return launch_staged<R, GAUGE, ALGO, 4>(c, e, a, sh.blocks_per_sm);
             }
         }
     }
@@ -1305,17 +1312,19 @@ int gf_autotune(gf_ctx *c, int *choice_fp32, int *choice_fp64)
     // prefetch); pipelined with 2, 4, 8 warps per block; (FP32 only) direct capped at 64 registers and
     // one thread per site (plain and pipelined).  Coulomb passes are direct only; refine-FP32 passes
     // (W tracking) are not the 4-lane pipelined one.
-    static const gf_ctx::PassShape cands64[] = {{0, 4, 0, 0}, {3, 4, 0, 0}, {6, 4, 0, 0}, {1, 4, 0, 1}, {1, 8, 0, 1},
-                                                {3, 4, 0, 1}, {1, 2, 0, 0}, {1, 4, 0, 0}, {1, 8, 0, 0}};
-    static const gf_ctx::PassShape cands32[] = {{0, 4, 0, 0}, {2, 4, 0, 0}, {3, 4, 0, 0}, {4, 4, 0, 0}, {5, 4, 0, 0},
-                                                {6, 4, 0, 0}, {7, 4, 0, 0}, {7, 4, 0, 1}, {3, 4, 0, 1},
-                                                {1, 2, 0, 0}, {1, 4, 0, 0}, {1, 8, 0, 0}};
+    static const gf_ctx::PassShape cands64[] = {{0, 4, 0, 0, 0}, {3, 4, 0, 0, 0}, {6, 4, 0, 0, 0}, {1, 4, 0, 1, 0},
+                                                {1, 8, 0, 1, 0}, {1, 4, 0, 1, 1}, {3, 4, 0, 1, 0}, {1, 2, 0, 0, 0},
+                                                {1, 4, 0, 0, 0}, {1, 8, 0, 0, 0}};
+    static const gf_ctx::PassShape cands32[] = {{0, 4, 0, 0, 0}, {2, 4, 0, 0, 0}, {3, 4, 0, 0, 0}, {4, 4, 0, 0, 0},
+                                                {5, 4, 0, 0, 0}, {6, 4, 0, 0, 0}, {7, 4, 0, 0, 0}, {7, 4, 0, 1, 0},
+                                                {7, 4, 0, 1, 1}, {3, 4, 0, 1, 0}, {1, 2, 0, 0, 0}, {1, 4, 0, 0, 0},
+                                                {1, 8, 0, 0, 0}};
     for (int prec = 0; prec < 2; prec++) {
         if (prec == 0 && !c->mixed) continue;
         const gf_ctx::PassShape *cands = prec == 0 ? cands32 : cands64;
-        int ncand = prec == 0 ? 12 : 9;
+        int ncand = prec == 0 ? 13 : 10;
         if (c->gauge == GF_COULOMB) ncand = 1;
-        else if (prec == 0 && c->site_w) ncand = 9;
+        else if (prec == 0 && c->site_w) ncand = 10;
         // scratch field, descriptors and states for this precision
         const InstDesc &last = c->h_inst.back();
         const size_t span32 = (size_t)(reinterpret_cast<const char *>(last.f32 ? last.f32 : (float4 *)nullptr) -
@@ -1401,7 +1410,7 @@ int gf_autotune(gf_ctx *c, int *choice_fp32, int *choice_fp64)
         c->drop_graphs();
     }
     auto code = [](const gf_ctx::PassShape &sh) {
-        return (sh.alternate ? 1000 : 0) + (sh.variant == 1 ? sh.warps
+        return (sh.capped ? 10000 : 0) + (sh.alternate ? 1000 : 0) + (sh.variant == 1 ? sh.warps
                : sh.variant == 2 ? 64
                : sh.variant == 3 ? 100
                : sh.variant == 4 ? 32
@@ -1434,22 +1443,26 @@ int gf_set_pass_shape(gf_ctx *c, int real, int variant, int warps)
     c->shape[real].variant = variant;
     c->shape[real].warps = warps;
     c->shape[real].alternate = 0;
+    c->shape[real].capped = 0;
     c->shape[real].blocks_per_sm = 0;
     c->tuned[real] = 1;
     return GF_OK;
 }
 
 // Walk order of the persistent parity passes (variants 1, 3 and 7): alternate = 1 walks the tiles of
-// odd-parity passes backwards, so every pass starts on the links the previous one touched last.
-int gf_set_pass_order(gf_ctx *c, int real, int alternate)
+// odd-parity passes backwards, so every pass starts on the links the previous one touched last;
+// capped = 1 caps the registers of variants 1 (4 warps per block: 128) and 7 (170) so that more
+// warps are resident.
+int gf_set_pass_order(gf_ctx *c, int real, int alternate, int capped)
 {
     clear_error();
-    if (!c || !valid_real(real) || (alternate != 0 && alternate != 1)) {
+    if (!c || !valid_real(real) || (alternate != 0 && alternate != 1) || (capped != 0 && capped != 1)) {
         set_error("invalid argument to gf_set_pass_order");
         return GF_ERR_INVALID;
     }
     c->drop_graphs();
     c->shape[real].alternate = alternate;
+    c->shape[real].capped = capped;
     return GF_OK;
 }
 

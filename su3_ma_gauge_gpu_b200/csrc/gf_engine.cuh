@@ -426,8 +426,8 @@ __device__ __forceinline__ void fetch_pair_regs(const EngineDev &e, const InstCa
     }
 }
 
-template <typename R, int GAUGE, int ALGO, bool SITE_W>
-__global__ void __launch_bounds__(128) k_batched_pass_pair_rp(EngineDev e, int64_t total_tiles, int parity,
+template <typename R, int GAUGE, int ALGO, bool SITE_W, int MINB = 1>
+__global__ void __launch_bounds__(128, MINB) k_batched_pass_pair_rp(EngineDev e, int64_t total_tiles, int parity,
                                                               AlgoParams p, int want_state, int reverse)
 {
     static_assert(GAUGE != COULOMB, "Coulomb slices use k_batched_pass");
@@ -897,8 +897,8 @@ __device__ __forceinline__ void unstage_link(const uint4 *stage, int first, Link
     reconstruct(L);
 }
 
-template <typename R, int GAUGE, int ALGO, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) k_batched_pass_staged(EngineDev e, int64_t total_warps, int parity,
+template <typename R, int GAUGE, int ALGO, int WARPS, int MINB = 1>
+__global__ void __launch_bounds__(WARPS * 32, MINB) k_batched_pass_staged(EngineDev e, int64_t total_warps, int parity,
                                                                       AlgoParams p, int want_state, int reverse)
 {
     extern __shared__ uint4 smem[];

@@ -202,10 +202,11 @@ class GaugeFixer:
         r = _lib.GF_FP64 if real in ("fp64", "double") else _lib.GF_FP32
         check(lib().gf_set_pass_shape(self._h, r, variant, warps), "gf_set_pass_shape")
 
-    def set_pass_order(self, real: str, alternate: bool) -> None:
-        """Persistent passes: walk odd-parity passes backwards (L2 reuse between passes)."""
+    def set_pass_order(self, real: str, alternate: bool, capped: bool = False) -> None:
+        """Persistent passes: walk odd-parity passes backwards (L2 reuse between passes); capped:
+        fewer registers for more resident warps."""
         r = _lib.GF_FP64 if real in ("fp64", "double") else _lib.GF_FP32
-        check(lib().gf_set_pass_order(self._h, r, int(bool(alternate))), "gf_set_pass_order")
+        check(lib().gf_set_pass_order(self._h, r, int(bool(alternate)), int(bool(capped))), "gf_set_pass_order")
 
     def kernel_launches(self) -> int:
         n = ctypes.c_longlong()

@@ -383,17 +383,17 @@ def test_pipelined_pass_bit_identical_to_direct(cuda, prec):
     mixed = {"fp32": True, "fp64": False, "refine": "refine"}[prec]
     outs = {}
     if prec == "refine":
-        shapes = [(0, 4), (2, 4), (3, 4), (4, 4), (5, 4), (6, 4), (7, 4), (7, 4, 1), (3, 4, 1)]
+        shapes = [(0, 4), (2, 4), (3, 4), (4, 4), (5, 4), (6, 4), (7, 4), (7, 4, 1), (3, 4, 1), (7, 4, 1, 1)]
     else:
-        shapes = [(0, 4), (1, 2), (1, 4), (1, 8), (3, 4), (6, 4), (1, 4, 1), (1, 8, 1), (3, 4, 1)] + (
-            [(2, 4), (4, 4), (5, 4), (7, 4), (7, 4, 1)] if prec == "fp32" else [])
+        shapes = [(0, 4), (1, 2), (1, 4), (1, 8), (3, 4), (6, 4), (1, 4, 1), (1, 8, 1), (3, 4, 1), (1, 4, 1, 1)] + (
+            [(2, 4), (4, 4), (5, 4), (7, 4), (7, 4, 1), (7, 4, 1, 1)] if prec == "fp32" else [])
     for shape in shapes:
         variant, warps = shape[:2]
         with GaugeFixer(sizes, mixed=mixed) as gf:
             real = "fp64" if prec == "fp64" else "fp32"
             gf.set_pass_shape(real, variant, warps)
             if len(shape) > 2:
-                gf.set_pass_order(real, True)
+                gf.set_pass_order(real, True, len(shape) > 3)
             for i, U in enumerate(fields):
                 gf.load(i, U)
             gf.sweeps("or", 4, 1.7)
@@ -485,6 +485,7 @@ def test_autotune_picks_a_shape(cuda):
         c32, c64 = gf.autotune()
         # codes + 1000: the same shape with the alternating walk (gf_set_pass_order)
         assert c32 % 1000 in (0, 64, 100, 32, 33, 16, 116, 2, 4, 8) and c64 % 1000 in (0, 100, 16, 2, 4, 8)
+        assert c32 < 20000 and c64 < 20000
         after = np.zeros_like(U)
         gf.store(0, after)
         assert np.array_equal(before, after)  # tuning ran on a scratch copy
