@@ -121,16 +121,57 @@ __global__ void __launch_bounds__(128) k_parity_pass_range(F f, Geom g, int pari
 }
 
 // ---- gauge quality ---------------------------------------------------------------------------
-template <typename R, class F>
-__device__ __forceinline__ void load_link_f64(const F &f, int64_t s, int mu, Link<double> &L)
+template <typename R>
+__device__ __forceinline__ void rows_f64(const R r[12], Link<double> &L)
 {
-    R r[12];
-    f.load12(s, mu, r);
     double d[12];
 #pragma unroll
     for (int k = 0; k < 12; k++) d[k] = (double)r[k];
     unpack12(L, d);
     reconstruct(L);
+}
+
+template <typename R, class F>
+__device__ __forceinline__ void load_link_f64(const F &f, int64_t s, int mu, Link<double> &L)
+{
+    R r[12];
+    f.load12(s, mu, r);
+    rows_f64(r, L);
+}
+
+// Visit the up link U_mu(x), then the down link U_mu(x - mu), of every direction mu >= mu0, in
+// FP64, in the order mu = mu0 .. 3 (so the arithmetic of the visitors runs in that order).  FP32
+// fields load the rows of all these links (at most 96 floats) before any arithmetic, so the eight
+// loads of a site are in flight together; FP64 fields load one link at a time.
+template <typename R, int MU0, class F, class Up, class Down>
+__device__ __forceinline__ void visit_site_links(const F &f, const Geom &g, int64_t s, const int32_t c[4], Up up,
+                                                 Down down)
+{
+    if constexpr (sizeof(R) == 4) {
+        R ru[4][12], rd[4][12];
+#pragma unroll
+        for (int mu = MU0; mu < 4; mu++) {
+            f.load12(s, mu, ru[mu]);
+            f.load12(neighbour_down(g, c, mu), mu, rd[mu]);
+        }
+#pragma unroll
+        for (int mu = MU0; mu < 4; mu++) {
+            Link<double> u;
+            rows_f64(ru[mu], u);
+            up(u);
+            rows_f64(rd[mu], u);
+            down(u);
+        }
+    } else {
+#pragma unroll 1
+        for (int mu = MU0; mu < 4; mu++) {
+            Link<double> u;
+            load_link_f64<R>(f, s, mu, u);
+            up(u);
+            load_link_f64<R>(f, neighbour_down(g, c, mu), mu, u);
+            down(u);
+        }
+    }
 }
 
 // Per-site functional and theta, computed in FP64 from the stored rows:
@@ -147,11 +188,8 @@ __device__ __forceinline__ void quality_site(const F &f, const Geom &g, int64_t 
     gff = 0;
     if (GAUGE == MAG) {
         double X[3][2] = {{0, 0}, {0, 0}, {0, 0}};
-#pragma unroll 1
-        for (int mu = 0; mu < 4; mu++) {
-            Link<double> u, d;
-            load_link_f64<R>(f, s, mu, u);
-            load_link_f64<R>(f, neighbour_down(g, c, mu), mu, d);
+        Link<double> u;
+        visit_site_links<R, 0>(f, g, s, c, [&](const Link<double> &l) { u = l; }, [&](const Link<double> &d) {
             gff += abs2(u.e[0][0]) + abs2(u.e[1][1]) + abs2(u.e[2][2]);
 #pragma unroll
             for (int k = 0; k < 3; k++) {
@@ -165,7 +203,7 @@ __device__ __forceinline__ void quality_site(const F &f, const Geom &g, int64_t 
                 X[k][0] += (p.x * q.x + p.y * q.y) - (r.x * t.x + r.y * t.y);
                 X[k][1] += (p.x * q.y - p.y * q.x) - (r.x * t.y - r.y * t.x);
             }
-        }
+        });
         th = sqrt(X[0][0] * X[0][0] + X[0][1] * X[0][1]) + sqrt(X[1][0] * X[1][0] + X[1][1] * X[1][1]) +
              sqrt(X[2][0] * X[2][0] + X[2][1] * X[2][1]);
     } else {
@@ -174,28 +212,27 @@ __device__ __forceinline__ void quality_site(const F &f, const Geom &g, int64_t 
         for (int i = 0; i < 3; i++)
 #pragma unroll
             for (int j = 0; j < 3; j++) D[i][j] = cx<double>(0, 0);
-        const int mu0 = GAUGE == COULOMB ? 1 : 0;
-#pragma unroll 1
-        for (int mu = mu0; mu < 4; mu++) {
-            Link<double> u;
-            load_link_f64<R>(f, s, mu, u);
-            gff += u.e[0][0].x + u.e[1][1].x + u.e[2][2].x;
+        visit_site_links<R, GAUGE == COULOMB ? 1 : 0>(
+            f, g, s, c,
+            [&](const Link<double> &u) {
+                gff += u.e[0][0].x + u.e[1][1].x + u.e[2][2].x;
 #pragma unroll
-            for (int i = 0; i < 3; i++)
+                for (int i = 0; i < 3; i++)
 #pragma unroll
-                for (int j = 0; j < 3; j++) {
-                    D[i][j].x += u.e[i][j].x;
-                    D[i][j].y += u.e[i][j].y;
-                }
-            load_link_f64<R>(f, neighbour_down(g, c, mu), mu, u);
+                    for (int j = 0; j < 3; j++) {
+                        D[i][j].x += u.e[i][j].x;
+                        D[i][j].y += u.e[i][j].y;
+                    }
+            },
+            [&](const Link<double> &d) {
 #pragma unroll
-            for (int i = 0; i < 3; i++)
+                for (int i = 0; i < 3; i++)
 #pragma unroll
-                for (int j = 0; j < 3; j++) {
-                    D[i][j].x -= u.e[i][j].x;
-                    D[i][j].y -= u.e[i][j].y;
-                }
-        }
+                    for (int j = 0; j < 3; j++) {
+                        D[i][j].x -= d.e[i][j].x;
+                        D[i][j].y -= d.e[i][j].y;
+                    }
+            });
         const double trx = (D[0][0].x + D[1][1].x + D[2][2].x) / 3.0;
         const double try_ = (D[0][0].y + D[1][1].y + D[2][2].y) / 3.0;
 #pragma unroll
