@@ -299,6 +299,21 @@ __global__ void __launch_bounds__(128, MINB) k_batched_pass_site(EngineDev e, in
     }
 }
 
+// cp.async: 16-byte copies bypass L1 (.cg); 8-byte copies must go through it (.ca)
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
 // ---- two lanes per site --------------------------------------------------------------------------
 // A warp updates 16 sites: lanes 0-7 and 16-23 the sites of 8-site tile 2T, lanes 8-15 and 24-31
 // those of tile 2T + 1.  Lane `role` = lane >> 4 of a site holds directions 2 role and 2 role + 1
@@ -389,17 +404,19 @@ __global__ void __launch_bounds__(128, MINB) k_batched_pass_pair(EngineDev e, in
 }
 
 // Persistent form with register prefetch: each warp walks a strided list of 16-site pair tiles and
-// loads the next one's links (and W column) into registers before it updates the current one.
+// loads the next one's links into registers before it updates the current one.  In refine mode the
+// next tile's W column goes to shared memory instead (cp.async, two stages per warp), which keeps
+// its registers free for the occupancy the register cap buys.
 template <typename R>
 struct PairRegs {
     PairSite ps;
     R up[2][12], dn[2][12];
-    float2 w[3];
 };
 
 template <typename R, bool SITE_W>
 __device__ __forceinline__ void fetch_pair_regs(const EngineDev &e, const InstCache &ic, int64_t tile,
-                                                int64_t total_tiles, int parity, int want_state, PairRegs<R> &t)
+                                                int64_t total_tiles, int parity, int want_state, PairRegs<R> &t,
+                                                float2 *wstage)
 {
     t.ps.inst = -1;
     if (tile >= total_tiles) return;
@@ -421,8 +438,9 @@ __device__ __forceinline__ void fetch_pair_regs(const EngineDev &e, const InstCa
         f.load12(t.ps.sd[j], 2 * role + j, t.dn[j]);
     }
     if (SITE_W) {
+        const int lane = threadIdx.x & 31;
 #pragma unroll
-        for (int r = 0; r < 3; r++) t.w[r] = d.w[(int64_t)(role * 3 + r) * d.g.V + t.ps.s];
+        for (int r = 0; r < 3; r++) cp_async8(wstage + r * 32 + lane, d.w + (int64_t)(role * 3 + r) * d.g.V + t.ps.s);
     }
 }
 
@@ -432,23 +450,33 @@ __global__ void __launch_bounds__(128, MINB) k_batched_pass_pair_rp(EngineDev e,
 {
     static_assert(GAUGE != COULOMB, "Coulomb slices use k_batched_pass");
     __shared__ InstCache ic;
+    // refine: this warp's two stages of the W column, [warp][stage][r][lane] (each lane reads back
+    // only what it copied, so the per-thread cp.async.wait_group is the only synchronisation)
+    __shared__ float2 wst[SITE_W ? 4 * 2 * 3 * 32 : 1];
     fill_inst_cache(e, ic);
     const int lane = threadIdx.x & 31, role = lane >> 4, half = (lane >> 3) & 1;
     const int64_t npair = (total_tiles + 1) / 2;                 // 16-site pair tiles
     const int64_t stride = (int64_t)gridDim.x * 4;
     int64_t pt = (int64_t)blockIdx.x * 4 + (threadIdx.x >> 5);   // this warp's pair tile
+    float2 *const wbase = wst + (SITE_W ? (threadIdx.x >> 5) * 2 * 3 * 32 : 0);
+    int wcur = 0;
     PairRegs<R> cur;
     cur.ps.inst = -1;
     if (pt < npair)
         fetch_pair_regs<R, SITE_W>(e, ic, ordered_tile(pt, npair, reverse) * 2 + half, total_tiles, parity, want_state,
-                                   cur);
+                                   cur, wbase);
+    if (SITE_W) cp_async_commit();
     // every lane of a warp runs the same iterations (pt is warp-uniform), so the shuffles are safe
     for (; pt < npair; pt += stride) {
         PairRegs<R> nxt;
         nxt.ps.inst = -1;
         if (pt + stride < npair)
             fetch_pair_regs<R, SITE_W>(e, ic, ordered_tile(pt + stride, npair, reverse) * 2 + half, total_tiles, parity,
-                                       want_state, nxt);
+                                       want_state, nxt, wbase + (wcur ^ 1) * 3 * 32);
+        if (SITE_W) {
+            cp_async_commit();
+            cp_async_wait<1>();  // this lane's W column of the current tile has landed
+        }
         const int i = cur.ps.inst;
         if (__any_sync(0xffffffffu, i >= 0)) {
             Link<R> up[2], dn[2];
@@ -468,8 +496,13 @@ __global__ void __launch_bounds__(128, MINB) k_batched_pass_pair_rp(EngineDev e,
                 }
             }
 #pragma unroll
-            for (int r = 0; r < 3; r++)
-                wcol[r] = (SITE_W && i >= 0) ? cx<R>((R)cur.w[r].x, (R)cur.w[r].y) : cx<R>((R)0, (R)0);
+            for (int r = 0; r < 3; r++) {
+                wcol[r] = cx<R>((R)0, (R)0);
+                if (SITE_W && i >= 0) {
+                    const float2 v = wbase[wcur * 3 * 32 + r * 32 + lane];
+                    wcol[r] = cx<R>((R)v.x, (R)v.y);
+                }
+            }
             Rng<R> rng;
             if (ALGO == ALG_SA || ALGO == ALG_SR || ALGO == ALG_RANDOM)
                 rng.init(ref_rng_tid(cur.ps.h), inst_seed(p, i < 0 ? 0 : i), inst_counter(p, i < 0 ? 0 : i));
@@ -491,7 +524,9 @@ __global__ void __launch_bounds__(128, MINB) k_batched_pass_pair_rp(EngineDev e,
             }
         }
         cur = nxt;
+        wcur ^= 1;
     }
+    if (SITE_W) cp_async_wait<0>();
 }
 
 // ---- refine mode: FP64 master + FP32 working copy + accumulated W --------------------------------
@@ -828,14 +863,6 @@ struct Chunks {
     static constexpr int per_lane = 2 * per_link;
 };
 
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
-{
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 struct TileRef {
     int inst;      // -1: nothing to do
@@ -957,12 +984,6 @@ struct SiteStage {
     static constexpr int slots = 24 + (SITE_W ? 3 : 0);
     static constexpr size_t bytes = (size_t)2 * slots * 128 * 16;
 };
-
-__device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
-{
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
-}
 
 template <bool SITE_W>
 __device__ __forceinline__ void prefetch_site(const EngineDev &e, const InstCache &ic, int i, int64_t h, int parity,
