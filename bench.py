@@ -280,13 +280,15 @@ def reference_gpu_leg(dU_in, gpu_id, fixes) -> dict | None:
 
 def run_profile_target(nsweeps: int, mode: str = "fast"):
     """A short, fixed launch sequence of the hot kernels for ncu (see profiles/): the 32^4 input,
-    `nsweeps` OR sweeps per launch shape in FP32, then the same in FP64 (shape = (variant, walk
-    order), gf_set_pass_shape / gf_set_pass_order).
+    `nsweeps` OR sweeps per launch shape in FP32, then the same in FP64 (shape = (variant, order):
+    gf_set_pass_shape, and gf_set_pass_order with alternate = order & 1, capped = order >> 1).
     mode "fast": FP32 storage; FP32 shapes direct, pipelined, two lanes per site (direct, register
-    prefetch, register prefetch with alternating walk); FP64 direct, pipelined (alternating walk).
+    prefetch, register prefetch with alternating walk, the same register-capped); FP64 direct,
+    pipelined (alternating walk).
     mode "refine": FP64 master + FP32 working copy with W; FP32 shapes direct, 64-register, register
     prefetch, thread per site (plain, pipelined), two lanes per site (direct, register prefetch, with
-    alternating walk); then FP64 direct, pipelined (4 warps; with alternating walk), register prefetch."""
+    alternating walk, the same register-capped); then FP64 direct, pipelined (4 warps; with
+    alternating walk), register prefetch."""
     import torch
 
     from su3_ma_gauge_gpu_b200 import synthetic as S
@@ -295,18 +297,18 @@ def run_profile_target(nsweeps: int, mode: str = "fast"):
     dU, _ = S.smooth_config(SIZE, EPS, 1234, device="cuda", as_tensor=True)
     torch.cuda.empty_cache()  # keep the device footprint of the profiled launches small
     if mode == "fast":
-        shapes = {"fp32": [(0, 0), (1, 0), (6, 0), (7, 0), (7, 1)], "fp64": [(0, 0), (1, 0), (1, 1)]}
+        shapes = {"fp32": [(0, 0), (1, 0), (6, 0), (7, 0), (7, 1), (7, 3)], "fp64": [(0, 0), (1, 0), (1, 1)]}
     else:
-        shapes = {"fp32": [(0, 0), (2, 0), (3, 0), (4, 0), (5, 0), (6, 0), (7, 0), (7, 1)],
+        shapes = {"fp32": [(0, 0), (2, 0), (3, 0), (4, 0), (5, 0), (6, 0), (7, 0), (7, 1), (7, 3)],
                   "fp64": [(0, 0), (1, 0), (1, 1), (3, 0)]}
     with GaugeFixer([SIZE], mixed=True if mode == "fast" else "refine") as gf:
         gf.load(0, dU)
         for real in ("fp32", "fp64"):
             if real == "fp64":
                 gf.to_fp64()
-            for variant, alt in shapes[real]:
+            for variant, order in shapes[real]:
                 gf.set_pass_shape(real, variant, 4)
-                gf.set_pass_order(real, bool(alt))
+                gf.set_pass_order(real, bool(order & 1), bool(order >> 1))
                 gf.sweeps("or", nsweeps, 1.7)
         g, a = gf.quality()
         gf.store(0, dU)

@@ -1107,8 +1107,8 @@ __global__ void __launch_bounds__(128, 2) k_batched_pass_site_staged(EngineDev e
 // barrier in ChunkSync and leaves the kernel, and every other block leaves at its next wait, so the
 // host gets an error status (GF_ERR_TIMEOUT) and the context stays usable.
 struct ChunkSync {
-    unsigned int count;   // blocks arrived at the current barrier
-    unsigned int gen;     // barrier generation
+    unsigned int count;   // barrier arrivals since the launch (zeroed before it; only grows)
+    unsigned int unused;
     unsigned int error;   // 1: a wait ran out of its budget
     unsigned int where;   // index of that barrier
 };
@@ -1125,29 +1125,40 @@ __device__ __forceinline__ unsigned long long global_ns()
     return t;
 }
 
-// Thread 0 of each block arrives; the last to arrive resets the count and opens the next
-// generation.  `arrivals` is the number of blocks the barrier waits for (gridDim.x; more only
-// when a test makes the wait run out).  Returns false when the block must leave the kernel.
+__device__ __forceinline__ unsigned int ld_acquire_gpu(const unsigned int *p)
+{
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void red_release_add_gpu(unsigned int *p, unsigned int v)
+{
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Grid barrier `index` (0, 1, 2, ... within a launch): thread 0 of each block adds its arrival to
+// the counter with release semantics (after the block's bar.sync, so it publishes every thread's
+// writes of the pass) and polls the counter with acquire loads until all `arrivals` blocks have
+// arrived at this barrier, count >= (index + 1) * arrivals.  One L2 round trip after the last
+// arrival releases everyone: no reset, no generation word, no full fences.  `arrivals` is
+// gridDim.x (more only when a test makes the wait run out).  The wait is bounded: a block that
+// waits longer than budget_ns records the barrier and leaves, and every other block leaves at its
+// next poll of the error word.  Returns false when the block must leave the kernel.
 __device__ __forceinline__ bool grid_barrier(ChunkSync *sy, unsigned int arrivals, unsigned long long budget_ns,
                                              unsigned int index)
 {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        volatile unsigned int *vgen = &sy->gen;
-        volatile unsigned int *verr = &sy->error;
         ok = 1;
-        const unsigned int g = *vgen;
-        __threadfence();
-        if (atomicAdd(&sy->count, 1u) == arrivals - 1) {
-            atomicExch(&sy->count, 0u);
-            __threadfence();
-            atomicAdd(&sy->gen, 1u);
-        } else {
+        const unsigned int target = (index + 1) * arrivals;
+        red_release_add_gpu(&sy->count, 1u);
+        if (ld_acquire_gpu(&sy->count) < target) {
             const unsigned long long t0 = global_ns();
-            for (unsigned int spin = 0; *vgen == g; spin++) {
-                if ((spin & 31u) != 31u) continue;  // poll the generation; the error word and the clock less often
-                if (*verr) {
+            for (unsigned int spin = 1; ld_acquire_gpu(&sy->count) < target; spin++) {
+                if (spin & 31u) continue;  // poll the counter; the error word and the clock less often
+                if (ld_acquire_gpu(&sy->error)) {
                     ok = 0;
                     break;
                 }
@@ -1158,8 +1169,7 @@ __device__ __forceinline__ bool grid_barrier(ChunkSync *sy, unsigned int arrival
                 }
             }
         }
-        __threadfence();
-        if (*verr) ok = 0;
+        if (ok && ld_acquire_gpu(&sy->error)) ok = 0;  // another block gave up: leave with it
     }
     __syncthreads();
     return ok != 0;
@@ -1187,15 +1197,25 @@ __global__ void __launch_bounds__(128) k_chunk_sweeps(EngineDev e, int64_t total
                                                       int want_state, ChunkSync *sy, unsigned int arrivals,
                                                       unsigned long long budget_ns)
 {
+    // the states cannot change inside a chunk (only its check moves them), so the descriptors and
+    // states of the first instances are read once per launch instead of once per tile and pass
+    __shared__ InstCache ic;
+    fill_inst_cache(e, ic);
     const int64_t wstride = (int64_t)gridDim.x * 4;
     const int64_t wfirst = (int64_t)blockIdx.x * 4 + (threadIdx.x >> 5);
     unsigned int bar = 0;
     for (int k = 0; k < nsweeps; k++) {
         for (int parity = 0; parity < 2; parity++) {
             for (int64_t warp = wfirst; warp < total_warps; warp += wstride) {
-                const int i = find_instance(e.inst, e.ninst, warp, [](const InstDesc &d) { return d.warp_begin; });
-                if (e.state[i] != want_state) continue;  // warp-uniform: a tile lies in one instance
-                const InstDesc d = e.inst[i];
+                int i;
+                if (e.ninst <= kInstCache) {
+                    i = find_instance(ic.d, ic.n, warp, [](const InstDesc &d) { return d.warp_begin; });
+                    if (ic.state[i] != want_state) continue;  // warp-uniform: a tile lies in one instance
+                } else {
+                    i = find_instance(e.inst, e.ninst, warp, [](const InstDesc &d) { return d.warp_begin; });
+                    if (e.state[i] != want_state) continue;
+                }
+                const InstDesc &d = inst_at(e, ic, i);
                 const PackedFieldL2<R> f = packed_l2_of<R>(d);
                 parity_pass_warp<R, GAUGE, ALG_OR, PackedFieldL2<R>, GAUGE == COULOMB, false>(
                     f, f, d.g, warp - d.warp_begin, parity, p, nullptr);
@@ -1206,9 +1226,11 @@ __global__ void __launch_bounds__(128) k_chunk_sweeps(EngineDev e, int64_t total
         if (repro.after(k)) {
             for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total_links;
                  idx += (int64_t)gridDim.x * blockDim.x) {
-                const int i = find_instance(e.inst, e.ninst, idx, [](const InstDesc &d) { return d.link_begin; });
-                if (e.state[i] != want_state) continue;
-                const InstDesc d = e.inst[i];
+                const int i = e.ninst <= kInstCache
+                                  ? find_instance(ic.d, ic.n, idx, [](const InstDesc &d) { return d.link_begin; })
+                                  : find_instance(e.inst, e.ninst, idx, [](const InstDesc &d) { return d.link_begin; });
+                if ((i < ic.n ? ic.state[i] : e.state[i]) != want_state) continue;
+                const InstDesc &d = inst_at(e, ic, i);
                 const int64_t l = idx - d.link_begin;
                 const int mu = (int)(l / d.g.V);
                 const int64_t s = l - mu * d.g.V;
