@@ -48,6 +48,8 @@ BYTES_PER_SITE_UPDATE = {"fp32": 768, "fp64": 1536, "fp32_refine": 768 + 96}
 
 def pass_kernel_name(code: int, real: str, refine: bool) -> str:
     """The OR-pass kernel an autotuner choice stands for (gf_autotune's output codes)."""
+    if code >= 100000:
+        return pass_kernel_name(code - 100000, real, refine) + ", three cp.async stages"
     if code >= 10000:
         return pass_kernel_name(code - 10000, real, refine) + ", registers capped"
     if code >= 1000:
@@ -73,12 +75,15 @@ def pass_kernel_name(code: int, real: str, refine: bool) -> str:
 
 def apply_pass_code(gf, real: str, code: int) -> None:
     """Set the OR-pass launch shape an autotuner code stands for (gf_autotune's output codes)."""
+    stages3, code = code >= 100000, code % 100000
     capped, code = code >= 10000, code % 10000
     alternate, code = code >= 1000, code % 1000
     variant, warps = {0: (0, 4), 64: (2, 4), 100: (3, 4), 32: (4, 4), 33: (5, 4), 16: (6, 4), 116: (7, 4),
                       2: (1, 2), 4: (1, 4), 8: (1, 8)}[code]
     gf.set_pass_shape(real, variant, warps)
     gf.set_pass_order(real, alternate, capped)
+    if stages3:
+        gf.set_pass_stages(real, 3)
 
 
 def env_rank():

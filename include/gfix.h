@@ -271,7 +271,8 @@ int gf_fix(gf_ctx *ctx, const gf_schedule *schedule, gf_report *reports);
  * 64 = direct with 64 registers, 100 = register prefetch, 32 = thread per site, 33 = thread per site
  * pipelined with cp.async, 2/4/8 = warps per block of the pipelined pass, 16 = two lanes per site,
  * 116 = two lanes per site with register prefetch, each + 1000 when the passes alternate their walk
- * order and + 10000 with capped registers (gf_set_pass_order) (-1: precision not used). */
+ * order, + 10000 with capped registers (gf_set_pass_order) and + 100000 with three cp.async stages
+ * (gf_set_pass_stages) (-1: precision not used). */
 int gf_autotune(gf_ctx *ctx, int *choice_fp32, int *choice_fp64);
 /* Fix the launch shape instead: variant 0 (direct), 1 (pipelined, warps = 2, 4 or 8), 2 (FP32
  * direct capped at 64 registers), 3 (register prefetch), 4 (FP32, one thread per site), 5 (FP32,
@@ -284,6 +285,11 @@ int gf_set_pass_shape(gf_ctx *ctx, int real, int variant, int warps);
  * previous pass touched last and still finds them in L2; capped = 1 caps the registers of variants 1
  * (4 warps per block) and 7 so that more warps are resident.  gf_set_pass_shape resets both to 0. */
 int gf_set_pass_order(gf_ctx *ctx, int real, int alternate, int capped);
+/* cp.async stages per warp of the pipelined pass (variant 1 with 4 warps per block): 2 (default)
+ * keeps the next 8-site tile in flight while the current one is computed, 3 the next two (twice the
+ * bytes in flight for the same resident warps; the FP64 pass's choice on a B200).  GF_ERR_INVALID
+ * for 3 with any other launch shape; gf_set_pass_shape resets it to 2. */
+int gf_set_pass_stages(gf_ctx *ctx, int real, int stages);
 /* Number of instances (lattices, or timeslices for GF_COULOMB). */
 int gf_instances(gf_ctx *ctx);
 /* The OR checks of the last gf_fix with schedule.trace_checks > 0: for instance `instance`, up to

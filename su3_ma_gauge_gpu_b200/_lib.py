@@ -107,6 +107,7 @@ SIGNATURES.update({
     "gf_autotune": (_c_int, [_vp, ctypes.POINTER(_c_int), ctypes.POINTER(_c_int)]),
     "gf_set_pass_shape": (_c_int, [_vp, _c_int, _c_int, _c_int]),
     "gf_set_pass_order": (_c_int, [_vp, _c_int, _c_int, _c_int]),
+    "gf_set_pass_stages": (_c_int, [_vp, _c_int, _c_int]),
     "gf_instances": (_c_int, [_vp]),
 })
 

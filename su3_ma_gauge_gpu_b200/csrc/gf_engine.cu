@@ -103,6 +103,7 @@ struct gf_ctx {
         int variant = 0, warps = 4, blocks_per_sm = 0;
         int alternate = 0;  // persistent variants (1, 3, 7): walk the tiles backwards on odd parities
         int capped = 0;     // variants 1 (4 warps per block) and 7: registers capped for more resident warps
+        int stages = 2;     // variant 1 with 4 warps per block: cp.async stages per warp (2 or 3)
     } shape[2];
     int tuned[2] = {0, 0};
     // the lattices the caller passed: first instance and number of instances (Coulomb contexts
@@ -150,11 +151,11 @@ struct PassArgs {
     int reverse;  // persistent passes: walk the tiles backwards
 };
 
-template <typename R, int GAUGE, int ALGO, int WARPS, int MINB = 1>
+template <typename R, int GAUGE, int ALGO, int WARPS, int MINB = 1, int STAGES = 2>
 int launch_staged(const gf_ctx *c, const EngineDev &e, const PassArgs &a, int blocks_per_sm)
 {
-    const size_t smem = staged_smem_bytes<R>(WARPS);
-    auto kern = k_batched_pass_staged<R, GAUGE, ALGO, WARPS, MINB>;
+    const size_t smem = staged_smem_bytes<R>(WARPS, STAGES);
+    auto kern = k_batched_pass_staged<R, GAUGE, ALGO, WARPS, MINB, STAGES>;
     static bool smem_opt_in = false;  // above 48 KB the dynamic shared memory must be opted in
     if (!smem_opt_in) {
         int st = cuda_status(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
@@ -299,6 +300,7 @@ int launch_pass(const gf_ctx *c, const EngineDev &e, const PassArgs &a, const gf
             case 2: return launch_staged<R, GAUGE, ALGO, 2>(c, e, a, sh.blocks_per_sm);
             case 8: return launch_staged<R, GAUGE, ALGO, 8>(c, e, a, sh.blocks_per_sm);
             default:
+                if (sh.stages == 3) return launch_staged<R, GAUGE, ALGO, 4, 1, 3>(c, e, a, sh.blocks_per_sm);
                 if (sh.capped) return launch_staged<R, GAUGE, ALGO, 4, 4>(c, e, a, sh.blocks_per_sm);  // 128 registers
                 return launch_staged<R, GAUGE, ALGO, 4>(c, e, a, sh.blocks_per_sm);
             }
@@ -1312,9 +1314,9 @@ int gf_autotune(gf_ctx *c, int *choice_fp32, int *choice_fp64)
     // prefetch); pipelined with 2, 4, 8 warps per block; (FP32 only) direct capped at 64 registers and
     // one thread per site (plain and pipelined).  Coulomb passes are direct only; refine-FP32 passes
     // (W tracking) are not the 4-lane pipelined one.
-    static const gf_ctx::PassShape cands64[] = {{0, 4, 0, 0, 0}, {3, 4, 0, 0, 0}, {6, 4, 0, 0, 0}, {1, 4, 0, 1, 0},
-                                                {1, 8, 0, 1, 0}, {1, 4, 0, 1, 1}, {3, 4, 0, 1, 0}, {1, 2, 0, 0, 0},
-                                                {1, 4, 0, 0, 0}, {1, 8, 0, 0, 0}};
+    static const gf_ctx::PassShape cands64[] = {{0, 4, 0, 0, 0}, {3, 4, 0, 0, 0}, {6, 4, 0, 0, 0},    {1, 4, 0, 1, 0},
+                                                {1, 8, 0, 1, 0}, {1, 4, 0, 1, 1}, {3, 4, 0, 1, 0},    {1, 2, 0, 0, 0},
+                                                {1, 4, 0, 0, 0}, {1, 8, 0, 0, 0}, {1, 4, 0, 1, 0, 3}, {1, 4, 0, 0, 0, 3}};
     static const gf_ctx::PassShape cands32[] = {{0, 4, 0, 0, 0}, {2, 4, 0, 0, 0}, {3, 4, 0, 0, 0}, {4, 4, 0, 0, 0},
                                                 {5, 4, 0, 0, 0}, {6, 4, 0, 0, 0}, {7, 4, 0, 0, 0}, {7, 4, 0, 1, 0},
                                                 {7, 4, 0, 1, 1}, {3, 4, 0, 1, 0}, {1, 2, 0, 0, 0}, {1, 4, 0, 0, 0},
@@ -1322,7 +1324,7 @@ int gf_autotune(gf_ctx *c, int *choice_fp32, int *choice_fp64)
     for (int prec = 0; prec < 2; prec++) {
         if (prec == 0 && !c->mixed) continue;
         const gf_ctx::PassShape *cands = prec == 0 ? cands32 : cands64;
-        int ncand = prec == 0 ? 13 : 10;
+        int ncand = prec == 0 ? 13 : 12;
         if (c->gauge == GF_COULOMB) ncand = 1;
         else if (prec == 0 && c->site_w) ncand = 10;
         // scratch field, descriptors and states for this precision
@@ -1410,7 +1412,8 @@ int gf_autotune(gf_ctx *c, int *choice_fp32, int *choice_fp64)
         c->drop_graphs();
     }
     auto code = [](const gf_ctx::PassShape &sh) {
-        return (sh.capped ? 10000 : 0) + (sh.alternate ? 1000 : 0) + (sh.variant == 1 ? sh.warps
+        return (sh.stages == 3 ? 100000 : 0) + (sh.capped ? 10000 : 0) + (sh.alternate ? 1000 : 0) +
+               (sh.variant == 1 ? sh.warps
                : sh.variant == 2 ? 64
                : sh.variant == 3 ? 100
                : sh.variant == 4 ? 32
@@ -1444,6 +1447,7 @@ int gf_set_pass_shape(gf_ctx *c, int real, int variant, int warps)
     c->shape[real].warps = warps;
     c->shape[real].alternate = 0;
     c->shape[real].capped = 0;
+    c->shape[real].stages = 2;
     c->shape[real].blocks_per_sm = 0;
     c->tuned[real] = 1;
     return GF_OK;
@@ -1463,6 +1467,21 @@ int gf_set_pass_order(gf_ctx *c, int real, int alternate, int capped)
     c->drop_graphs();
     c->shape[real].alternate = alternate;
     c->shape[real].capped = capped;
+    return GF_OK;
+}
+
+// cp.async stages per warp of the pipelined pass (variant 1 with 4 warps per block): 2 keeps the
+// next tile in flight while the current one is computed, 3 the next two.
+int gf_set_pass_stages(gf_ctx *c, int real, int stages)
+{
+    clear_error();
+    if (!c || !valid_real(real) || (stages != 2 && stages != 3) ||
+        (stages == 3 && (c->shape[real].variant != 1 || c->shape[real].warps != 4))) {
+        set_error("invalid argument to gf_set_pass_stages (three stages: the pipelined pass with 4 warps per block)");
+        return GF_ERR_INVALID;
+    }
+    c->drop_graphs();
+    c->shape[real].stages = stages;
     return GF_OK;
 }
 

@@ -924,28 +924,35 @@ __device__ __forceinline__ void unstage_link(const uint4 *stage, int first, Link
     reconstruct(L);
 }
 
-template <typename R, int GAUGE, int ALGO, int WARPS, int MINB = 1>
+// STAGES = 2: the next tile is in flight while the current one is computed; STAGES = 3: the next two
+// (a ring of three stages per warp, twice the bytes in flight for the same warps).
+template <typename R, int GAUGE, int ALGO, int WARPS, int MINB = 1, int STAGES = 2>
 __global__ void __launch_bounds__(WARPS * 32, MINB) k_batched_pass_staged(EngineDev e, int64_t total_warps, int parity,
                                                                       AlgoParams p, int want_state, int reverse)
 {
+    static_assert(STAGES == 2 || STAGES == 3, "two or three stages");
     extern __shared__ uint4 smem[];
     constexpr int NCH = Chunks<R>::per_lane;
     const int w = threadIdx.x >> 5;
-    uint4 *const wbase = smem + (2 * w) * NCH * 32;  // this warp's two stages, NCH * 32 chunks apart
+    uint4 *const wbase = smem + (STAGES * w) * NCH * 32;  // this warp's stages, NCH * 32 chunks apart
     const int64_t stride = (int64_t)gridDim.x * WARPS;
     int64_t tile = (int64_t)blockIdx.x * WARPS + w;
-    int cur = 0;
-    TileRef t = tile < total_warps ? prefetch_tile<R>(e, ordered_tile(tile, total_warps, reverse), parity, want_state,
-                                                      wbase)
-                                   : TileRef{-1, 0, 0, 0};
-    cp_async_commit();
-    for (; tile < total_warps; tile += stride) {
-        const int64_t nt = tile + stride;
-        const TileRef n = nt < total_warps ? prefetch_tile<R>(e, ordered_tile(nt, total_warps, reverse), parity,
-                                                              want_state, wbase + (cur ^ 1) * NCH * 32)
+    // prefetch tile tt into stage st and close its cp.async group (an empty group past the end)
+    auto issue = [&](int64_t tt, int st) -> TileRef {
+        const TileRef r = tt < total_warps ? prefetch_tile<R>(e, ordered_tile(tt, total_warps, reverse), parity,
+                                                              want_state, wbase + st * NCH * 32)
                                            : TileRef{-1, 0, 0, 0};
         cp_async_commit();
-        cp_async_wait<1>();
+        return r;
+    };
+    int cur = 0;
+    TileRef t = issue(tile, 0);
+    TileRef t1{-1, 0, 0, 0};
+    if (STAGES == 3) t1 = issue(tile + stride, 1);
+    for (; tile < total_warps; tile += stride) {
+        // the stage consumed in the previous iteration receives the tile STAGES - 1 strides ahead
+        const TileRef n = issue(tile + (STAGES - 1) * stride, (cur + STAGES - 1) % STAGES);
+        cp_async_wait<STAGES - 1>();  // this tile's group (the oldest in flight) has landed
         if (t.inst >= 0) {
             const InstDesc &d = e.inst[t.inst];
             const int mu = (threadIdx.x & 31) >> 3;
@@ -961,16 +968,21 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) k_batched_pass_staged(Engine
             store_link<R>(f, t.sd, mu, dn);
         }
         __syncwarp();  // every lane is done with the current stage before it is refilled
-        t = n;
-        cur ^= 1;
+        if (STAGES == 3) {
+            t = t1;
+            t1 = n;
+        } else {
+            t = n;
+        }
+        cur = (cur + 1) % STAGES;
     }
     cp_async_wait<0>();
 }
 
 template <typename R>
-constexpr size_t staged_smem_bytes(int warps)
+constexpr size_t staged_smem_bytes(int warps, int stages = 2)
 {
-    return (size_t)warps * 2 * Chunks<R>::per_lane * 32 * 16;
+    return (size_t)warps * stages * Chunks<R>::per_lane * 32 * 16;
 }
 
 // ---- one thread per site, pipelined: FP32 only ---------------------------------------------------

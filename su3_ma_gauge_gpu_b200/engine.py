@@ -208,6 +208,11 @@ class GaugeFixer:
         r = _lib.GF_FP64 if real in ("fp64", "double") else _lib.GF_FP32
         check(lib().gf_set_pass_order(self._h, r, int(bool(alternate)), int(bool(capped))), "gf_set_pass_order")
 
+    def set_pass_stages(self, real: str, stages: int) -> None:
+        """Pipelined pass with 4 warps per block: cp.async stages per warp (2, or 3: two tiles in flight)."""
+        r = _lib.GF_FP64 if real in ("fp64", "double") else _lib.GF_FP32
+        check(lib().gf_set_pass_stages(self._h, r, stages), "gf_set_pass_stages")
+
     def kernel_launches(self) -> int:
         n = ctypes.c_longlong()
         check(lib().gf_kernel_launches(self._h, ctypes.byref(n)), "gf_kernel_launches")
