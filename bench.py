@@ -293,7 +293,8 @@ def run_profile_target(nsweeps: int, mode: str = "fast"):
     mode "refine": FP64 master + FP32 working copy with W; FP32 shapes direct, 64-register, register
     prefetch, thread per site (plain, pipelined), two lanes per site (direct, register prefetch, with
     alternating walk, the same register-capped); then FP64 direct, pipelined (4 warps; with
-    alternating walk), register prefetch."""
+    alternating walk; the same with three cp.async stages), register prefetch.  A third entry in a
+    shape is the stage count (gf_set_pass_stages)."""
     import torch
 
     from su3_ma_gauge_gpu_b200 import synthetic as S
@@ -305,15 +306,17 @@ def run_profile_target(nsweeps: int, mode: str = "fast"):
         shapes = {"fp32": [(0, 0), (1, 0), (6, 0), (7, 0), (7, 1), (7, 3)], "fp64": [(0, 0), (1, 0), (1, 1)]}
     else:
         shapes = {"fp32": [(0, 0), (2, 0), (3, 0), (4, 0), (5, 0), (6, 0), (7, 0), (7, 1), (7, 3)],
-                  "fp64": [(0, 0), (1, 0), (1, 1), (3, 0)]}
+                  "fp64": [(0, 0), (1, 0), (1, 1), (1, 1, 3), (3, 0)]}
     with GaugeFixer([SIZE], mixed=True if mode == "fast" else "refine") as gf:
         gf.load(0, dU)
         for real in ("fp32", "fp64"):
             if real == "fp64":
                 gf.to_fp64()
-            for variant, order in shapes[real]:
+            for variant, order, *stages in shapes[real]:
                 gf.set_pass_shape(real, variant, 4)
                 gf.set_pass_order(real, bool(order & 1), bool(order >> 1))
+                if stages:
+                    gf.set_pass_stages(real, stages[0])
                 gf.sweeps("or", nsweeps, 1.7)
         g, a = gf.quality()
         gf.store(0, dU)
