@@ -312,13 +312,14 @@ def test_reference_kernel_timing(cuda):
         stream = torch.cuda.Stream()
         gf = GaugeFixer([size], mixed=(prec == "f32"), stream=stream)
         gf.load(0, dU)
+        c32, c64 = gf.autotune()  # the launch shape a fix would use
         torch.cuda.synchronize()
         t_packed = time_it(lambda: gf.sweeps("or", 1, 1.7), stream=stream)
         gf.close()
         gbs = lambda t: 192 * nb * V / (t * 1e-3) / 1e9  # noqa: E731
         out[prec] = {"ref_ms_per_sweep": t_ref, "ref_GBs": gbs(t_ref), "plugin_ms_per_sweep": t_plugin,
                      "plugin_GBs": gbs(t_plugin), "packed_ms_per_sweep": t_packed, "packed_GBs": gbs(t_packed),
-                     "speedup_packed_vs_ref": t_ref / t_packed}
+                     "packed_shape": c32 if prec == "f32" else c64, "speedup_packed_vs_ref": t_ref / t_packed}
     print(json.dumps(out))
     path = os.environ.get("GF_REF_TIMING_OUT")
     if path:
