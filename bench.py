@@ -283,6 +283,29 @@ def reference_gpu_leg(dU_in, gpu_id, fixes) -> dict | None:
     return out
 
 
+def run_profile_target_sa(nsweeps: int):
+    """A short launch sequence of the MAG heat-bath pass for ncu: the MAG 48^4 workload's field
+    construction at 32^4 (U = exp(i*0.5*H) under a Haar gauge transform) in a refine context,
+    `nsweeps` SA sweeps at T = 0.7 with the two-lane direct pass (the shape SA runs with when the
+    OR pass is the two-lane register-prefetch one), then with one thread per site."""
+    import torch
+
+    from su3_ma_gauge_gpu_b200 import synthetic as S
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer
+
+    dU, _ = S.smooth_config(SIZE, 0.5, 4849, device="cuda", as_tensor=True)
+    torch.cuda.empty_cache()
+    with GaugeFixer([SIZE], gauge="mag", mixed="refine") as gf:
+        gf.load(0, dU)
+        for variant in (6, 4):
+            gf.set_pass_shape("fp32", variant, 4)
+            gf.sweeps("sa", nsweeps, 0.7, 9, 1)
+        g, a = gf.quality()
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_target": "ok", "mode": "mag-sa", "sweeps_per_shape": nsweeps, "F": float(g[0]),
+                      "theta": float(a[0])}))
+
+
 def run_profile_target(nsweeps: int, mode: str = "fast"):
     """A short, fixed launch sequence of the hot kernels for ncu (see profiles/): the 32^4 input,
     `nsweeps` OR sweeps per launch shape in FP32, then the same in FP64 (shape = (variant, order):
@@ -622,7 +645,7 @@ def main():
     ap.add_argument("--extras", default="all",
                     help="comma-separated configurations to run after the headline on a single GPU and report as "
                          "extra keys (plain8, coulomb48x16, gribov64, mag48), 'all' or 'none'")
-    ap.add_argument("--profile-mode", default="fast", choices=["fast", "refine"])
+    ap.add_argument("--profile-mode", default="fast", choices=["fast", "refine", "mag-sa"])
     ap.add_argument("--pass-fp32", type=int, default=None, help="launch-list mode: FP32 pass shape (autotuner code)")
     ap.add_argument("--pass-fp64", type=int, default=None, help="launch-list mode: FP64 pass shape (autotuner code)")
     ap.add_argument("--launch-list", action="store_true",
@@ -635,7 +658,10 @@ def main():
         run_reference(args)
         return
     if args.profile:
-        run_profile_target(args.profile, args.profile_mode)
+        if args.profile_mode == "mag-sa":
+            run_profile_target_sa(args.profile)
+        else:
+            run_profile_target(args.profile, args.profile_mode)
         return
     if args.launch_list:
         run_launch_list(args)
