@@ -133,7 +133,10 @@ __device__ __forceinline__ void right_mult(Link<R> &L, const R h[4])
 }
 
 // ---- Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11) ---------------------------------------
-__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k)
+// Not inlined: a heat-bath site update draws from up to eight call sites per subgroup, three
+// subgroups per update, and inlined copies of the ten rounds made the kernel's code outgrow the
+// instruction cache (the SA pass stalled on instruction fetch more than on anything else).
+static __device__ __noinline__ uint4 philox4x32_10(uint4 c, uint2 k)
 {
 #pragma unroll
     for (int r = 0; r < 10; r++) {
