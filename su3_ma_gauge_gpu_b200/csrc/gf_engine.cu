@@ -286,9 +286,9 @@ int launch_pass(const gf_ctx *c, const EngineDev &e, const PassArgs &a, const gf
             return launch_status("batched parity pass (thread per site)");
         }
     }
-    if constexpr (ALGO == ALG_OR && GAUGE != COULOMB) {
-        if (sh.variant == 3) {
-            if constexpr (sizeof(R) == 4) {
+    if constexpr (ALGO == ALG_OR) {
+        if (sh.variant == 3) {  // also Coulomb slices (their W rides in the temporal planes)
+            if constexpr (sizeof(R) == 4 && GAUGE != COULOMB) {
                 if (c->site_w) return launch_rp<R, GAUGE, ALGO, true>(c, e, a, sh.blocks_per_sm);
             }
             return launch_rp<R, GAUGE, ALGO, false>(c, e, a, sh.blocks_per_sm);
@@ -1312,7 +1312,7 @@ int gf_autotune(gf_ctx *c, int *choice_fp32, int *choice_fp64)
     if (st) return st;
     // direct; register prefetch (persistent); two lanes per site (direct, and persistent with register
     // prefetch); pipelined with 2, 4, 8 warps per block; (FP32 only) direct capped at 64 registers and
-    // one thread per site (plain and pipelined).  Coulomb passes are direct only; refine-FP32 passes
+    // one thread per site (plain and pipelined).  Coulomb passes are direct or register prefetch; refine-FP32 passes
     // (W tracking) are not the 4-lane pipelined one.
     static const gf_ctx::PassShape cands64[] = {{0, 4, 0, 0, 0}, {3, 4, 0, 0, 0}, {6, 4, 0, 0, 0},    {1, 4, 0, 1, 0},
                                                 {1, 8, 0, 1, 0}, {1, 4, 0, 1, 1}, {3, 4, 0, 1, 0},    {1, 2, 0, 0, 0},
@@ -1321,11 +1321,13 @@ int gf_autotune(gf_ctx *c, int *choice_fp32, int *choice_fp64)
                                                 {5, 4, 0, 0, 0}, {6, 4, 0, 0, 0}, {7, 4, 0, 0, 0}, {7, 4, 0, 1, 0},
                                                 {7, 4, 0, 1, 1}, {3, 4, 0, 1, 0}, {1, 2, 0, 0, 0}, {1, 4, 0, 0, 0},
                                                 {1, 8, 0, 0, 0}};
+    // Coulomb slices: direct, and register prefetch with and without the alternating walk
+    static const gf_ctx::PassShape candsC[] = {{0, 4, 0, 0, 0}, {3, 4, 0, 0, 0}, {3, 4, 0, 1, 0}};
     for (int prec = 0; prec < 2; prec++) {
         if (prec == 0 && !c->mixed) continue;
-        const gf_ctx::PassShape *cands = prec == 0 ? cands32 : cands64;
+        const gf_ctx::PassShape *cands = c->gauge == GF_COULOMB ? candsC : prec == 0 ? cands32 : cands64;
         int ncand = prec == 0 ? 13 : 12;
-        if (c->gauge == GF_COULOMB) ncand = 1;
+        if (c->gauge == GF_COULOMB) ncand = 3;
         else if (prec == 0 && c->site_w) ncand = 10;
         // scratch field, descriptors and states for this precision
         const InstDesc &last = c->h_inst.back();
@@ -1443,10 +1445,11 @@ int gf_set_pass_shape(gf_ctx *c, int real, int variant, int warps)
 {
     clear_error();
     if (!c || !valid_real(real) || variant < 0 || variant > 7 || (warps != 2 && warps != 4 && warps != 8) ||
-        (variant != 0 && variant != 2 && c->gauge == GF_COULOMB) || (variant == 1 && real == GF_FP32 && c->site_w) ||
+        (variant != 0 && variant != 2 && variant != 3 && c->gauge == GF_COULOMB) ||
+        (variant == 1 && real == GF_FP32 && c->site_w) ||
         ((variant == 2 || variant == 4 || variant == 5) && real == GF_FP64)) {
-        set_error("invalid pass shape (Coulomb passes are direct or 64-register; refine-FP32 passes are not "
-                  "pipelined; the 64-register and thread-per-site passes are FP32)");
+        set_error("invalid pass shape (Coulomb passes are direct, 64-register or register prefetch; refine-FP32 "
+                  "passes are not pipelined; the 64-register and thread-per-site passes are FP32)");
         return GF_ERR_INVALID;
     }
     c->drop_graphs();

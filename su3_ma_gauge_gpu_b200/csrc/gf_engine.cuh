@@ -143,7 +143,9 @@ __device__ __forceinline__ int site_of(const EngineDev &e, const InstCache &ic, 
 // Persistent variant with register prefetch: every warp walks a strided list of 8-site tiles and
 // issues the loads of tile t+1 (its lane's two links, and the W column in refine mode) into
 // registers before it computes tile t, so each warp keeps a tile's worth of loads in flight
-// through its arithmetic and shuffles.  Same site update as k_batched_pass; not for COULOMB.
+// through its arithmetic and shuffles.  Same site update as k_batched_pass.  COULOMB slices: the
+// mu = 0 lane holds the slice's W (its temporal plane) as its up link and has no down link, as in
+// parity_pass_warp.
 template <typename R>
 struct TileRegs {
     int inst;        // -1: nothing to do
@@ -152,7 +154,7 @@ struct TileRegs {
     float2 w[3];
 };
 
-template <typename R, bool SITE_W>
+template <typename R, int GAUGE, bool SITE_W>
 __device__ __forceinline__ void fetch_tile_regs(const EngineDev &e, const InstCache &ic, int64_t tile, int parity,
                                                 int want_state, TileRegs<R> &t)
 {
@@ -172,10 +174,11 @@ __device__ __forceinline__ void fetch_tile_regs(const EngineDev &e, const InstCa
     int32_t c[4];
     site_coords(d.g, t.h, parity, c);
     t.s = t.h + (parity ? d.g.Vh : 0);
-    t.sd = neighbour_down(d.g, c, mu);
+    const bool wlane = GAUGE == COULOMB && mu == 0;
+    t.sd = wlane ? t.s : neighbour_down(d.g, c, mu);
     const PackedField<R> f = packed_of<R>(d);
     f.load12(t.s, mu, t.up);
-    f.load12(t.sd, mu, t.dn);
+    if (!wlane) f.load12(t.sd, mu, t.dn);
     if (SITE_W) {
         const int k = mu & 1;
 #pragma unroll
@@ -187,29 +190,37 @@ template <typename R, int GAUGE, int ALGO, bool SITE_W>
 __global__ void __launch_bounds__(128) k_batched_pass_rp(EngineDev e, int64_t total_warps, int parity, AlgoParams p,
                                                          int want_state, int reverse)
 {
-    static_assert(GAUGE != COULOMB, "Coulomb slices use k_batched_pass");
+    static_assert(GAUGE != COULOMB || !SITE_W, "Coulomb slices carry W in their temporal planes");
     __shared__ InstCache ic;
     fill_inst_cache(e, ic);
     const int mu = (threadIdx.x & 31) >> 3;
+    const bool wlane = GAUGE == COULOMB && mu == 0;
     const int64_t stride = (int64_t)gridDim.x * 4;
     int64_t tile = (int64_t)blockIdx.x * 4 + (threadIdx.x >> 5);
     TileRegs<R> cur;
     cur.inst = -1;
     if (tile < total_warps)
-        fetch_tile_regs<R, SITE_W>(e, ic, ordered_tile(tile, total_warps, reverse), parity, want_state, cur);
+        fetch_tile_regs<R, GAUGE, SITE_W>(e, ic, ordered_tile(tile, total_warps, reverse), parity, want_state, cur);
     for (; tile < total_warps; tile += stride) {
         TileRegs<R> nxt;
         nxt.inst = -1;
         if (tile + stride < total_warps)
-            fetch_tile_regs<R, SITE_W>(e, ic, ordered_tile(tile + stride, total_warps, reverse), parity, want_state,
-                                       nxt);
+            fetch_tile_regs<R, GAUGE, SITE_W>(e, ic, ordered_tile(tile + stride, total_warps, reverse), parity,
+                                              want_state, nxt);
         if (cur.inst >= 0) {
             const InstDesc &d = inst_at(e, ic, cur.inst);
             Link<R> up, dn;
             unpack12(up, cur.up);
             reconstruct(up);
-            unpack12(dn, cur.dn);
-            reconstruct(dn);
+            if (wlane) {  // the slice's W rides as the up link; no down link
+#pragma unroll
+                for (int a = 0; a < 3; a++)
+#pragma unroll
+                    for (int b = 0; b < 3; b++) dn.e[a][b] = cx<R>(a == b ? (R)1 : (R)0, (R)0);
+            } else {
+                unpack12(dn, cur.dn);
+                reconstruct(dn);
+            }
             Rng<R> rng;
             if (ALGO == ALG_SA || ALGO == ALG_SR || ALGO == ALG_RANDOM)
                 rng.init(ref_rng_tid(cur.h), inst_seed(p, cur.inst), inst_counter(p, cur.inst));
@@ -221,7 +232,7 @@ __global__ void __launch_bounds__(128) k_batched_pass_rp(EngineDev e, int64_t to
             site_update<GAUGE, ALGO, R, SITE_W>(up, dn, mu, p, rng, &wcol);
             const PackedField<R> f = packed_of<R>(d);
             store_link<R>(f, cur.s, mu, up);
-            store_link<R>(f, cur.sd, mu, dn);
+            if (!wlane) store_link<R>(f, cur.sd, mu, dn);
             if (SITE_W && mu < 2) {
 #pragma unroll
                 for (int r = 0; r < 3; r++)

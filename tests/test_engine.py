@@ -412,6 +412,38 @@ def test_pipelined_pass_bit_identical_to_direct(cuda, prec):
             assert np.array_equal(res[i], base[i]), (key, i)
 
 
+@pytest.mark.parametrize("mixed", [False, True, "refine"], ids=["fp64", "fp32", "refine"])
+def test_coulomb_register_prefetch_pass_bit_identical_to_direct(cuda, mixed):
+    """Coulomb slices on the persistent register-prefetch pass (variant 3, with and without the
+    alternating walk): the temporal lane carries the slice's W as its up link and has no down link,
+    as in the direct pass, so OR sweeps are bit for bit the direct pass's; the export applies W to
+    the temporal links, so W is compared too."""
+    from su3_ma_gauge_gpu_b200.engine import GaugeFixer
+
+    sizes = [(4, 4, 6, 4), (2, 8, 4, 4)]
+    fields = [np.concatenate([S.smooth_config((1,) + s[1:], 0.3, 190 + 10 * i + t)[0] for t in range(s[0])])
+              for i, s in enumerate(sizes)]
+    real = "fp64" if mixed is False else "fp32"
+    outs = {}
+    for variant, alternate in ((0, False), (3, False), (3, True)):
+        with GaugeFixer(sizes, gauge="coulomb", mixed=mixed) as gf:
+            gf.set_pass_shape(real, variant, 4)
+            gf.set_pass_order(real, alternate)
+            for i, U in enumerate(fields):
+                gf.load(i, U)
+            gf.sweeps("or", 4, 1.7)
+            res = []
+            for i, U in enumerate(fields):
+                o = np.zeros_like(U)
+                gf.store(i, o)
+                res.append(o)
+            outs[(variant, alternate)] = res
+    base = outs[(0, False)]
+    for key, res in outs.items():
+        for i in range(len(sizes)):
+            assert np.array_equal(res[i], base[i]), (key, i)
+
+
 def test_pass_stages_need_the_four_warp_pipelined_pass(cuda):
     """Three cp.async stages exist for the pipelined pass with 4 warps per block only; any other
     shape, or a stage count other than 2 or 3, is refused."""
