@@ -56,6 +56,13 @@ int make_geom(const int32_t size[4], int gauge, bool plugin_slice, Geom &g)
         set_error("lattice volume %lld exceeds 2^31 sites", (long long)V);
         return GF_ERR_INVALID;
     }
+    // a warp updates an 8-site tile of one parity; four even extents always give V % 16 == 0, three
+    // (a Coulomb timeslice) may not (6^3: 108 sites per parity).  The reference's kernels need a
+    // whole number of 32-site blocks per parity (apps/CoulombGaugeFixingSU3_4D.cu:138).
+    if ((V / 2) % 8 != 0) {
+        set_error("volume %lld: each parity must hold a multiple of 8 sites (V %% 16 == 0)", (long long)V);
+        return GF_ERR_INVALID;
+    }
     g.V = V;
     g.Vh = V / 2;
     geom_init_div(g);

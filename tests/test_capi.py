@@ -84,5 +84,10 @@ def test_context_parameter_checks_without_gpu():
     assert b"Nt = 3" in L.gf_last_error_string()
     p = _lib.CtxParams(gauge=_lib.GF_LANDAU, ninstances=1, sizes=sizes, mixed=3, stream=None)
     assert L.gf_create(ctypes.byref(p), ctypes.byref(h)) == _lib.GF_ERR_INVALID
+    # a 6^3 timeslice has 108 sites per parity, not a whole number of 8-site tiles
+    slice6 = (ctypes.c_int32 * 4)(2, 6, 6, 6)
+    p = _lib.CtxParams(gauge=_lib.GF_COULOMB, ninstances=1, sizes=slice6, mixed=0, stream=None)
+    assert L.gf_create(ctypes.byref(p), ctypes.byref(h)) == _lib.GF_ERR_INVALID
+    assert b"multiple of 8 sites" in L.gf_last_error_string()
     p = _lib.CtxParams(gauge=_lib.GF_LANDAU, ninstances=0, sizes=sizes, mixed=0, stream=None)
     assert L.gf_create(ctypes.byref(p), ctypes.byref(h)) == _lib.GF_ERR_INVALID
