@@ -277,7 +277,7 @@ int gf_autotune(gf_ctx *ctx, int *choice_fp32, int *choice_fp64);
 /* Fix the launch shape instead: variant 0 (direct), 1 (pipelined, warps = 2, 4 or 8), 2 (FP32
  * direct capped at 64 registers), 3 (register prefetch), 4 (FP32, one thread per site), 5 (FP32,
  * one thread per site pipelined; OR, the other rules run as 4), 6 (two lanes per site) or 7 (two
- * lanes per site with register prefetch; OR, the other rules run as 6).  GF_COULOMB: 0, 2 or 3;
+ * lanes per site with register prefetch; OR, the other rules run as 6).  GF_COULOMB: 0, 2, 3, 6 or 7;
  * refine FP32: not 1. */
 int gf_set_pass_shape(gf_ctx *ctx, int real, int variant, int warps);
 /* Walk order and occupancy of the persistent passes (variants 1, 3, 7): alternate = 1 walks the

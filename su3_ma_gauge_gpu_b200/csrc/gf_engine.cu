@@ -239,34 +239,41 @@ int launch_pair_rp(const gf_ctx *c, const EngineDev &e, const PassArgs &a, int b
 template <typename R, int GAUGE, int ALGO>
 int launch_pass(const gf_ctx *c, const EngineDev &e, const PassArgs &a, const gf_ctx::PassShape &sh)
 {
-    if constexpr (GAUGE != COULOMB) {
-        // two lanes per site: 7 = persistent with register prefetch (OR), 6 = direct (every rule,
-        // and the other rules when 7 is chosen)
-        if constexpr (ALGO == ALG_OR && sizeof(R) == 4) {  // FP64 would spill at 255 registers
-            if (sh.variant == 7) {
-                if (sh.capped) {  // 170 registers: 3 blocks of 4 warps per SM instead of 2
-                    if (c->site_w) return launch_pair_rp<R, GAUGE, ALGO, true, 3>(c, e, a, sh.blocks_per_sm);
-                    return launch_pair_rp<R, GAUGE, ALGO, false, 3>(c, e, a, sh.blocks_per_sm);
+    // two lanes per site: 7 = persistent with register prefetch (OR), 6 = direct (every rule, and
+    // the other rules when 7 is chosen); Coulomb slices too (no W tracking: theirs rides in the
+    // temporal planes)
+    if constexpr (ALGO == ALG_OR && sizeof(R) == 4) {  // FP64 would spill at 255 registers
+        if (sh.variant == 7) {
+            if constexpr (GAUGE != COULOMB) {
+                if (c->site_w) {
+                    if (sh.capped) return launch_pair_rp<R, GAUGE, ALGO, true, 3>(c, e, a, sh.blocks_per_sm);
+                    return launch_pair_rp<R, GAUGE, ALGO, true>(c, e, a, sh.blocks_per_sm);
                 }
-                if (c->site_w) return launch_pair_rp<R, GAUGE, ALGO, true>(c, e, a, sh.blocks_per_sm);
-                return launch_pair_rp<R, GAUGE, ALGO, false>(c, e, a, sh.blocks_per_sm);
             }
+            // capped: 168 registers, 3 blocks of 4 warps per SM instead of 2
+            if (sh.capped) return launch_pair_rp<R, GAUGE, ALGO, false, 3>(c, e, a, sh.blocks_per_sm);
+            return launch_pair_rp<R, GAUGE, ALGO, false>(c, e, a, sh.blocks_per_sm);
         }
-        if (sh.variant == 6 || sh.variant == 7) {
-            const unsigned blocks = grid_for((a.c->total_warps + 1) / 2 * 32, 128);
-            if constexpr (sizeof(R) == 4) {
-                if (c->site_w)
+    }
+    if (sh.variant == 6 || sh.variant == 7) {
+        const unsigned blocks = grid_for((a.c->total_warps + 1) / 2 * 32, 128);
+        if constexpr (sizeof(R) == 4) {
+            bool done = false;
+            if constexpr (GAUGE != COULOMB) {
+                if (c->site_w) {
                     k_batched_pass_pair<R, GAUGE, ALGO, true, 4><<<blocks, 128, 0, a.c->stream>>>(
                         e, a.c->total_warps, a.parity, a.p, a.want_state);
-                else
-                    k_batched_pass_pair<R, GAUGE, ALGO, false, 4><<<blocks, 128, 0, a.c->stream>>>(
-                        e, a.c->total_warps, a.parity, a.p, a.want_state);
-            } else {
-                k_batched_pass_pair<R, GAUGE, ALGO, false, 2><<<blocks, 128, 0, a.c->stream>>>(
-                    e, a.c->total_warps, a.parity, a.p, a.want_state);
+                    done = true;
+                }
             }
-            return launch_status("batched parity pass (two lanes per site)");
+            if (!done)
+                k_batched_pass_pair<R, GAUGE, ALGO, false, 4><<<blocks, 128, 0, a.c->stream>>>(
+                    e, a.c->total_warps, a.parity, a.p, a.want_state);
+        } else {
+            k_batched_pass_pair<R, GAUGE, ALGO, false, 2><<<blocks, 128, 0, a.c->stream>>>(
+                e, a.c->total_warps, a.parity, a.p, a.want_state);
         }
+        return launch_status("batched parity pass (two lanes per site)");
     }
     if constexpr (sizeof(R) == 4 && GAUGE != COULOMB && ALGO == ALG_OR) {
         if (sh.variant == 5) {
@@ -1312,7 +1319,7 @@ int gf_autotune(gf_ctx *c, int *choice_fp32, int *choice_fp64)
     if (st) return st;
     // direct; register prefetch (persistent); two lanes per site (direct, and persistent with register
     // prefetch); pipelined with 2, 4, 8 warps per block; (FP32 only) direct capped at 64 registers and
-    // one thread per site (plain and pipelined).  Coulomb passes are direct or register prefetch; refine-FP32 passes
+    // one thread per site (plain and pipelined).  Coulomb passes are direct, register prefetch or two lanes per site; refine-FP32 passes
     // (W tracking) are not the 4-lane pipelined one.
     static const gf_ctx::PassShape cands64[] = {{0, 4, 0, 0, 0}, {3, 4, 0, 0, 0}, {6, 4, 0, 0, 0},    {1, 4, 0, 1, 0},
                                                 {1, 8, 0, 1, 0}, {1, 4, 0, 1, 1}, {3, 4, 0, 1, 0},    {1, 2, 0, 0, 0},
@@ -1321,13 +1328,16 @@ int gf_autotune(gf_ctx *c, int *choice_fp32, int *choice_fp64)
                                                 {5, 4, 0, 0, 0}, {6, 4, 0, 0, 0}, {7, 4, 0, 0, 0}, {7, 4, 0, 1, 0},
                                                 {7, 4, 0, 1, 1}, {3, 4, 0, 1, 0}, {1, 2, 0, 0, 0}, {1, 4, 0, 0, 0},
                                                 {1, 8, 0, 0, 0}};
-    // Coulomb slices: direct, and register prefetch with and without the alternating walk
-    static const gf_ctx::PassShape candsC[] = {{0, 4, 0, 0, 0}, {3, 4, 0, 0, 0}, {3, 4, 0, 1, 0}};
+    // Coulomb slices: direct; register prefetch with and without the alternating walk; two lanes per
+    // site (direct, register prefetch with the alternating walk, the same register-capped; the
+    // prefetching ones FP32 only, in FP64 they run as the direct one)
+    static const gf_ctx::PassShape candsC[] = {{0, 4, 0, 0, 0}, {3, 4, 0, 0, 0}, {3, 4, 0, 1, 0},
+                                               {6, 4, 0, 0, 0}, {7, 4, 0, 1, 0}, {7, 4, 0, 1, 1}};
     for (int prec = 0; prec < 2; prec++) {
         if (prec == 0 && !c->mixed) continue;
         const gf_ctx::PassShape *cands = c->gauge == GF_COULOMB ? candsC : prec == 0 ? cands32 : cands64;
         int ncand = prec == 0 ? 13 : 12;
-        if (c->gauge == GF_COULOMB) ncand = 3;
+        if (c->gauge == GF_COULOMB) ncand = prec == 0 ? 6 : 4;
         else if (prec == 0 && c->site_w) ncand = 10;
         // scratch field, descriptors and states for this precision
         const InstDesc &last = c->h_inst.back();
@@ -1445,11 +1455,11 @@ int gf_set_pass_shape(gf_ctx *c, int real, int variant, int warps)
 {
     clear_error();
     if (!c || !valid_real(real) || variant < 0 || variant > 7 || (warps != 2 && warps != 4 && warps != 8) ||
-        (variant != 0 && variant != 2 && variant != 3 && c->gauge == GF_COULOMB) ||
+        (variant != 0 && variant != 2 && variant != 3 && variant != 6 && variant != 7 && c->gauge == GF_COULOMB) ||
         (variant == 1 && real == GF_FP32 && c->site_w) ||
         ((variant == 2 || variant == 4 || variant == 5) && real == GF_FP64)) {
-        set_error("invalid pass shape (Coulomb passes are direct, 64-register or register prefetch; refine-FP32 "
-                  "passes are not pipelined; the 64-register and thread-per-site passes are FP32)");
+        set_error("invalid pass shape (Coulomb passes are direct, 64-register, register prefetch or two lanes per "
+                  "site; refine-FP32 passes are not pipelined; the 64-register and thread-per-site passes are FP32)");
         return GF_ERR_INVALID;
     }
     c->drop_graphs();

@@ -332,7 +332,17 @@ __device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
 // half the shuffles, the SU(2) update computed twice per site instead of four times, and each of
 // the two tracked columns of W updated by one lane.  A tile's two lanes of a site are lane and
 // lane ^ 16, always in the same tile, so an idle tile (past the end, or an instance in another
-// state) only ever exchanges with itself.  Not for COULOMB (its slices carry W in a link slot).
+// state) only ever exchanges with itself.  COULOMB slices: direction 0 of role 0 is the slice's W
+// (its temporal plane), held as the up link with the identity as its down link, which is neither
+// loaded nor stored (as in parity_pass_warp); refine mode keeps no separate W array there.
+template <typename R>
+__device__ __forceinline__ void set_identity(Link<R> &L)
+{
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+        for (int b = 0; b < 3; b++) L.e[a][b] = cx<R>(a == b ? (R)1 : (R)0, (R)0);
+}
 struct PairSite {
     int inst;           // -1: idle
     int64_t h, s, sd[2];
@@ -356,8 +366,9 @@ template <typename R, int GAUGE, int ALGO, bool SITE_W, int MINB>
 __global__ void __launch_bounds__(128, MINB) k_batched_pass_pair(EngineDev e, int64_t total_tiles, int parity,
                                                                  AlgoParams p, int want_state)
 {
-    static_assert(GAUGE != COULOMB, "Coulomb slices use k_batched_pass");
+    static_assert(GAUGE != COULOMB || !SITE_W, "Coulomb slices carry W in their temporal planes");
     const int lane = threadIdx.x & 31, role = lane >> 4;
+    const bool wlane = GAUGE == COULOMB && role == 0;  // its direction 0 is the slice's W
     const int64_t tile = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 2 + ((lane >> 3) & 1);
     int i = -1;
     if (tile < total_tiles) {
@@ -378,7 +389,10 @@ __global__ void __launch_bounds__(128, MINB) k_batched_pass_pair(EngineDev e, in
 #pragma unroll
         for (int j = 0; j < 2; j++) {
             load_link<R>(f, ps.s, 2 * role + j, up[j]);
-            load_link<R>(f, ps.sd[j], 2 * role + j, dn[j]);
+            if (wlane && j == 0)
+                set_identity(dn[j]);
+            else
+                load_link<R>(f, ps.sd[j], 2 * role + j, dn[j]);
         }
         if (SITE_W) {
 #pragma unroll
@@ -405,7 +419,7 @@ __global__ void __launch_bounds__(128, MINB) k_batched_pass_pair(EngineDev e, in
 #pragma unroll
     for (int j = 0; j < 2; j++) {
         store_link<R>(f, ps.s, 2 * role + j, up[j]);
-        store_link<R>(f, ps.sd[j], 2 * role + j, dn[j]);
+        if (!(wlane && j == 0)) store_link<R>(f, ps.sd[j], 2 * role + j, dn[j]);
     }
     if (SITE_W) {
 #pragma unroll
@@ -424,7 +438,7 @@ struct PairRegs {
     R up[2][12], dn[2][12];
 };
 
-template <typename R, bool SITE_W>
+template <typename R, int GAUGE, bool SITE_W>
 __device__ __forceinline__ void fetch_pair_regs(const EngineDev &e, const InstCache &ic, int64_t tile,
                                                 int64_t total_tiles, int parity, int want_state, PairRegs<R> &t,
                                                 float2 *wstage)
@@ -446,7 +460,7 @@ __device__ __forceinline__ void fetch_pair_regs(const EngineDev &e, const InstCa
 #pragma unroll
     for (int j = 0; j < 2; j++) {
         f.load12(t.ps.s, 2 * role + j, t.up[j]);
-        f.load12(t.ps.sd[j], 2 * role + j, t.dn[j]);
+        if (!(GAUGE == COULOMB && role == 0 && j == 0)) f.load12(t.ps.sd[j], 2 * role + j, t.dn[j]);
     }
     if (SITE_W) {
         const int lane = threadIdx.x & 31;
@@ -459,13 +473,14 @@ template <typename R, int GAUGE, int ALGO, bool SITE_W, int MINB = 1>
 __global__ void __launch_bounds__(128, MINB) k_batched_pass_pair_rp(EngineDev e, int64_t total_tiles, int parity,
                                                               AlgoParams p, int want_state, int reverse)
 {
-    static_assert(GAUGE != COULOMB, "Coulomb slices use k_batched_pass");
+    static_assert(GAUGE != COULOMB || !SITE_W, "Coulomb slices carry W in their temporal planes");
     __shared__ InstCache ic;
     // refine: this warp's two stages of the W column, [warp][stage][r][lane] (each lane reads back
     // only what it copied, so the per-thread cp.async.wait_group is the only synchronisation)
     __shared__ float2 wst[SITE_W ? 4 * 2 * 3 * 32 : 1];
     fill_inst_cache(e, ic);
     const int lane = threadIdx.x & 31, role = lane >> 4, half = (lane >> 3) & 1;
+    const bool wlane = GAUGE == COULOMB && role == 0;  // its direction 0 is the slice's W
     const int64_t npair = (total_tiles + 1) / 2;                 // 16-site pair tiles
     const int64_t stride = (int64_t)gridDim.x * 4;
     int64_t pt = (int64_t)blockIdx.x * 4 + (threadIdx.x >> 5);   // this warp's pair tile
@@ -474,16 +489,16 @@ __global__ void __launch_bounds__(128, MINB) k_batched_pass_pair_rp(EngineDev e,
     PairRegs<R> cur;
     cur.ps.inst = -1;
     if (pt < npair)
-        fetch_pair_regs<R, SITE_W>(e, ic, ordered_tile(pt, npair, reverse) * 2 + half, total_tiles, parity, want_state,
-                                   cur, wbase);
+        fetch_pair_regs<R, GAUGE, SITE_W>(e, ic, ordered_tile(pt, npair, reverse) * 2 + half, total_tiles, parity,
+                                          want_state, cur, wbase);
     if (SITE_W) cp_async_commit();
     // every lane of a warp runs the same iterations (pt is warp-uniform), so the shuffles are safe
     for (; pt < npair; pt += stride) {
         PairRegs<R> nxt;
         nxt.ps.inst = -1;
         if (pt + stride < npair)
-            fetch_pair_regs<R, SITE_W>(e, ic, ordered_tile(pt + stride, npair, reverse) * 2 + half, total_tiles, parity,
-                                       want_state, nxt, wbase + (wcur ^ 1) * 3 * 32);
+            fetch_pair_regs<R, GAUGE, SITE_W>(e, ic, ordered_tile(pt + stride, npair, reverse) * 2 + half, total_tiles,
+                                              parity, want_state, nxt, wbase + (wcur ^ 1) * 3 * 32);
         if (SITE_W) {
             cp_async_commit();
             cp_async_wait<1>();  // this lane's W column of the current tile has landed
@@ -497,8 +512,12 @@ __global__ void __launch_bounds__(128, MINB) k_batched_pass_pair_rp(EngineDev e,
                 if (i >= 0) {
                     unpack12(up[j], cur.up[j]);
                     reconstruct(up[j]);
-                    unpack12(dn[j], cur.dn[j]);
-                    reconstruct(dn[j]);
+                    if (wlane && j == 0) {
+                        set_identity(dn[j]);
+                    } else {
+                        unpack12(dn[j], cur.dn[j]);
+                        reconstruct(dn[j]);
+                    }
                 } else {
 #pragma unroll
                     for (int a = 0; a < 3; a++)
@@ -524,7 +543,7 @@ __global__ void __launch_bounds__(128, MINB) k_batched_pass_pair_rp(EngineDev e,
 #pragma unroll
                 for (int j = 0; j < 2; j++) {
                     store_link<R>(f, cur.ps.s, 2 * role + j, up[j]);
-                    store_link<R>(f, cur.ps.sd[j], 2 * role + j, dn[j]);
+                    if (!(wlane && j == 0)) store_link<R>(f, cur.ps.sd[j], 2 * role + j, dn[j]);
                 }
                 if (SITE_W) {
 #pragma unroll

@@ -415,9 +415,10 @@ def test_pipelined_pass_bit_identical_to_direct(cuda, prec):
 @pytest.mark.parametrize("mixed", [False, True, "refine"], ids=["fp64", "fp32", "refine"])
 def test_coulomb_register_prefetch_pass_bit_identical_to_direct(cuda, mixed):
     """Coulomb slices on the persistent register-prefetch pass (variant 3, with and without the
-    alternating walk): the temporal lane carries the slice's W as its up link and has no down link,
-    as in the direct pass, so OR sweeps are bit for bit the direct pass's; the export applies W to
-    the temporal links, so W is compared too."""
+    alternating walk) and on the two-lane passes (6; 7 with the walk, register-capped): the
+    temporal direction carries the slice's W as its up link and has no down link, as in the direct
+    pass, and the two-lane sum (0 + v1) + (v2 + v3) is the 4-lane butterfly's, so OR sweeps are bit
+    for bit the direct pass's; the export applies W to the temporal links, so W is compared too."""
     from su3_ma_gauge_gpu_b200.engine import GaugeFixer
 
     sizes = [(4, 4, 6, 4), (2, 8, 4, 4)]
@@ -425,10 +426,11 @@ def test_coulomb_register_prefetch_pass_bit_identical_to_direct(cuda, mixed):
               for i, s in enumerate(sizes)]
     real = "fp64" if mixed is False else "fp32"
     outs = {}
-    for variant, alternate in ((0, False), (3, False), (3, True)):
+    for variant, alternate, capped in ((0, False, False), (3, False, False), (3, True, False), (6, False, False),
+                                       (7, False, False), (7, True, False), (7, True, True)):
         with GaugeFixer(sizes, gauge="coulomb", mixed=mixed) as gf:
             gf.set_pass_shape(real, variant, 4)
-            gf.set_pass_order(real, alternate)
+            gf.set_pass_order(real, alternate, capped)
             for i, U in enumerate(fields):
                 gf.load(i, U)
             gf.sweeps("or", 4, 1.7)
@@ -437,8 +439,8 @@ def test_coulomb_register_prefetch_pass_bit_identical_to_direct(cuda, mixed):
                 o = np.zeros_like(U)
                 gf.store(i, o)
                 res.append(o)
-            outs[(variant, alternate)] = res
-    base = outs[(0, False)]
+            outs[(variant, alternate, capped)] = res
+    base = outs[(0, False, False)]
     for key, res in outs.items():
         for i in range(len(sizes)):
             assert np.array_equal(res[i], base[i]), (key, i)
