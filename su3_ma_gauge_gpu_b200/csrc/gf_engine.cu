@@ -1475,7 +1475,7 @@ int gf_set_pass_shape(gf_ctx *c, int real, int variant, int warps)
 
 // Walk order of the persistent parity passes (variants 1, 3 and 7): alternate = 1 walks the tiles of
 // odd-parity passes backwards, so every pass starts on the links the previous one touched last;
-// capped = 1 caps the registers of variants 1 (4 warps per block: 128) and 7 (170) so that more
+// capped = 1 caps the registers of variants 1 (4 warps per block: 128) and 7 (168) so that more
 // warps are resident.
 int gf_set_pass_order(gf_ctx *c, int real, int alternate, int capped)
 {
