@@ -87,6 +87,12 @@ int gf_random_trafo(int gauge, int real, void *U, void *Udw, const int32_t size[
  * interior runs while the boundary links are exchanged.  Philox as gf_sa_step. */
 int gf_step_slices(int gauge, int real, int algo, void *U, const int32_t size[4], int parity, float param,
                    int seed, int rng_counter, int t_begin, int t_end, void *stream);
+/* The same, with site h of the lattice drawing its random numbers as site h + rng_site_offset
+ * (parity-split order): a t-slab of a larger lattice passes the offset of its first owned
+ * timeslice, ((global t of local slice 0) x Vs / 2), so its heat bath draws the whole lattice's
+ * stream and SA over slabs equals SA on the whole lattice. */
+int gf_step_slices_at(int gauge, int real, int algo, void *U, const int32_t size[4], int parity, float param,
+                      int seed, int rng_counter, int t_begin, int t_end, long long rng_site_offset, void *stream);
 /* *KernelsSU3::generateGaugeQualityPerSite (LandauKernelsSU3.hxx:71-74): per-site functional
  * and theta terms into device arrays of V doubles (either may be NULL). */
 int gf_quality_per_site(int gauge, int real, const void *U, const int32_t size[4], double *dGff,

@@ -61,6 +61,14 @@ void orc_step_range_f64(double *Uup, double *Udw, const int32_t size[4], int gau
                         float param, uint32_t seed, uint32_t counter, int64_t h_lo, int64_t h_hi, int nthreads);
 void orc_step_range_f32(float *Uup, float *Udw, const int32_t size[4], int gauge, int algo, int parity,
                         float param, uint32_t seed, uint32_t counter, int64_t h_lo, int64_t h_hi, int nthreads);
+/* The same with site h drawing its random numbers as site h + rng_site_offset (a t-slab's sites
+ * draw the whole lattice's stream). */
+void orc_step_range_at_f64(double *Uup, double *Udw, const int32_t size[4], int gauge, int algo, int parity,
+                           float param, uint32_t seed, uint32_t counter, int64_t h_lo, int64_t h_hi,
+                           int64_t rng_site_offset, int nthreads);
+void orc_step_range_at_f32(float *Uup, float *Udw, const int32_t size[4], int gauge, int algo, int parity,
+                           float param, uint32_t seed, uint32_t counter, int64_t h_lo, int64_t h_hi,
+                           int64_t rng_site_offset, int nthreads);
 
 /* Gauge quality (a18, a19): per-site arrays (optional, may be NULL) and the normalised
  * functional and theta as GaugeFixingStats::generateGaugeQuality (GaugeFixingStats.hxx:186-232)

@@ -376,9 +376,12 @@ static void FN(subgroup)(MAT M[8], int i, int j, int gauge, int algo, float para
 }
 
 /* One parity pass (the apply() of LandauKernelsSU3.hxx:216-256, CoulombKernelsSU3.hxx:208-250,
- * MAGKernelsSU3.hxx:248-293, U1xU1KernelsSU3.hxx:216-256), serial over sites. */
-void FN(orc_step_range)(REAL *Uup, REAL *Udw, const int32_t size[4], int gauge, int algo, int parity,
-                        float param, uint32_t seed, uint32_t counter, int64_t h_lo, int64_t h_hi, int nthreads)
+ * MAGKernelsSU3.hxx:248-293, U1xU1KernelsSU3.hxx:216-256), serial over sites, over the sites h in
+ * [h_lo, h_hi) of the parity.  Site h draws its random numbers as site h + rng_site_offset of the
+ * lattice would: a part of a larger lattice (a t-slab) then draws the whole lattice's stream. */
+void FN(orc_step_range_at)(REAL *Uup, REAL *Udw, const int32_t size[4], int gauge, int algo, int parity,
+                           float param, uint32_t seed, uint32_t counter, int64_t h_lo, int64_t h_hi,
+                           int64_t rng_site_offset, int nthreads)
 {
     const int64_t V = (int64_t)size[0] * size[1] * size[2] * size[3];
     const int64_t Vh = V / 2;
@@ -406,7 +409,8 @@ void FN(orc_step_range)(REAL *Uup, REAL *Udw, const int32_t size[4], int gauge, 
         if (algo == ORC_SA || algo == ORC_SR || algo == ORC_RANDOM) {
             /* key of the (mu=0, up) thread: blockIdx.x*blockDim.x + threadIdx.x with
              * NSB = 32 sites and 256 threads per block (apps/Makefile:36) */
-            uint32_t tid = (uint32_t)((h / 32) * 256 + (h % 32));
+            const int64_t hr = h + rng_site_offset;
+            uint32_t tid = (uint32_t)((hr / 32) * 256 + (hr % 32));
             FN(rng_init)(&rng, tid, seed, counter);
         }
         /* SU3::perSubgroup (SU3.hxx:762-771): (0,2), (1,2), (0,1) */
@@ -415,6 +419,12 @@ void FN(orc_step_range)(REAL *Uup, REAL *Udw, const int32_t size[4], int gauge, 
         FN(subgroup)(M, 0, 1, gauge, algo, param, &rng);
         for (int k = 0; k < 8; k++) FN(store12)(arr[k], V, site[k], k & 3, &M[k]);
     }
+}
+
+void FN(orc_step_range)(REAL *Uup, REAL *Udw, const int32_t size[4], int gauge, int algo, int parity,
+                        float param, uint32_t seed, uint32_t counter, int64_t h_lo, int64_t h_hi, int nthreads)
+{
+    FN(orc_step_range_at)(Uup, Udw, size, gauge, algo, parity, param, seed, counter, h_lo, h_hi, 0, nthreads);
 }
 
 void FN(orc_step)(REAL *Uup, REAL *Udw, const int32_t size[4], int gauge, int algo, int parity,

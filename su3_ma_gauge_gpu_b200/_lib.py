@@ -43,6 +43,8 @@ SIGNATURES = {
     "gf_random_trafo": (_c_int, [_c_int, _c_int, _vp, _vp, _i32p, _c_int, _c_int, _c_int, _vp]),
     "gf_step_slices": (_c_int, [_c_int, _c_int, _c_int, _vp, _i32p, _c_int, _c_float, _c_int, _c_int, _c_int, _c_int,
                                 _vp]),
+    "gf_step_slices_at": (_c_int, [_c_int, _c_int, _c_int, _vp, _i32p, _c_int, _c_float, _c_int, _c_int, _c_int,
+                                   _c_int, ctypes.c_longlong, _vp]),
     "gf_quality_per_site": (_c_int, [_c_int, _c_int, _vp, _i32p, _vp, _vp, _vp]),
     "gf_quality_prefactor_gff": (_c_double, [_c_int]),
     "gf_quality_prefactor_a": (_c_double, [_c_int]),

@@ -87,7 +87,7 @@ __global__ void __launch_bounds__(128) k_parity_pass(F Fup, F Fdw, Geom g, int p
 // rank updates its interior slices with it while the boundary links are on their way.
 template <typename R, int GAUGE, int ALGO, class F>
 __global__ void __launch_bounds__(128) k_parity_pass_range(F f, Geom g, int parity, AlgoParams p, int64_t h_lo,
-                                                           int64_t h_hi)
+                                                           int64_t h_hi, int64_t rng_site_offset)
 {
     static_assert(GAUGE != COULOMB, "timeslice ranges are for the 4D gauges");
     const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -112,7 +112,8 @@ __global__ void __launch_bounds__(128) k_parity_pass_range(F f, Geom g, int pari
             for (int j = 0; j < 3; j++) up.e[i][j] = dn.e[i][j] = cx<R>((R)0, (R)0);
     }
     Rng<R> rng;
-    if (ALGO == ALG_SA || ALGO == ALG_SR || ALGO == ALG_RANDOM) rng.init(ref_rng_tid(h), p.seed, p.counter);
+    if (ALGO == ALG_SA || ALGO == ALG_SR || ALGO == ALG_RANDOM)
+        rng.init(ref_rng_tid(h + rng_site_offset), p.seed, p.counter);  // the whole lattice's stream for a part of it
     site_update<GAUGE, ALGO>(up, dn, mu, p, rng);
     if (active) {
         store_link<R>(f, s, mu, up);

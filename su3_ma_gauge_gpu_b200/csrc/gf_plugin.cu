@@ -128,6 +128,7 @@ static int plugin_step(int gauge, int real, int algo, void *U, void *Udw, const 
 struct RangeArgs {
     StepArgs a;
     int64_t h_lo, h_hi;
+    int64_t rng_site_offset;  // site h draws its random numbers as site h + rng_site_offset
 };
 
 template <int GAUGE, int ALGO>
@@ -143,8 +144,8 @@ struct RefStepRange {
             const int64_t warps = (r.h_hi - (r.h_lo & ~(int64_t)7) + 7) / 8;
             if (warps <= 0) return GF_OK;
             const unsigned blocks = (unsigned)((warps * 32 + 127) / 128);
-            k_parity_pass_range<R, GAUGE, ALGO, RefField<R>><<<blocks, 128, 0, r.a.stream>>>(fu, r.a.g, r.a.parity, r.a.p,
-                                                                                          r.h_lo, r.h_hi);
+            k_parity_pass_range<R, GAUGE, ALGO, RefField<R>><<<blocks, 128, 0, r.a.stream>>>(
+                fu, r.a.g, r.a.parity, r.a.p, r.h_lo, r.h_hi, r.rng_site_offset);
             return launch_status("parity pass over timeslices");
         }
     }
@@ -249,6 +250,12 @@ int gf_random_trafo(int gauge, int real, void *U, void *Udw, const int32_t size[
 int gf_step_slices(int gauge, int real, int algo, void *U, const int32_t size[4], int parity, float param, int seed,
                    int rng_counter, int t_begin, int t_end, void *stream)
 {
+    return gf_step_slices_at(gauge, real, algo, U, size, parity, param, seed, rng_counter, t_begin, t_end, 0, stream);
+}
+
+int gf_step_slices_at(int gauge, int real, int algo, void *U, const int32_t size[4], int parity, float param,
+                      int seed, int rng_counter, int t_begin, int t_end, long long rng_site_offset, void *stream)
+{
     clear_error();
     if (!valid_gauge(gauge) || gauge == GF_COULOMB || !valid_real(real) || !U || (parity != 0 && parity != 1) ||
         algo < ALG_OR || algo > ALG_RANDOM) {
@@ -265,6 +272,11 @@ int gf_step_slices(int gauge, int real, int algo, void *U, const int32_t size[4]
     const int64_t half_slice = r.a.g.V / size[0] / 2;
     r.h_lo = t_begin * half_slice;
     r.h_hi = t_end * half_slice;
+    r.rng_site_offset = rng_site_offset;
+    if (r.h_lo + rng_site_offset < 0) {
+        set_error("rng_site_offset %lld puts site %lld before the lattice", rng_site_offset, (long long)r.h_lo);
+        return GF_ERR_INVALID;
+    }
     r.a.real = real;
     r.a.U = U;
     r.a.Udw = U;

@@ -31,9 +31,11 @@ is posted without waiting -- the next pass waits for it only before it updates t
 The halo sites themselves are never updated.  With NCCL the waits are stream dependencies, so the
 host never blocks inside a sweep.
 
-The functional and theta are summed with all_reduce.  Only deterministic updates
-(overrelaxation, microcanonical) give the single-lattice result bit for bit: the heat-bath draws
-its Philox numbers by local site index.
+The functional and theta are summed with all_reduce.  Every update rule gives the single-lattice
+result bit for bit: overrelaxation and microcanonical steps are deterministic, and the random ones
+(heat bath, stochastic relaxation, random transformations) draw each site's Philox numbers by its
+index in the whole lattice -- in the parity-split order a slab's sites are the global ones shifted
+by one constant, `TSlab.rng_site_offset`, which gf_step_slices_at takes.
 """
 from __future__ import annotations
 
@@ -76,6 +78,9 @@ class TSlab:
         self._owned_global = _site_index(self.size, tl - 2 + self.t0, xx, yy, zz)
         self._owned_mask = np.zeros(V, dtype=bool)
         self._owned_mask[self._owned_local] = True
+        # local site h (either parity) is global site h + rng_site_offset: local slice t is global
+        # slice t0 - 2 + t, and in the parity-split order a slice holds Vs / 2 sites of each parity
+        self.rng_site_offset = (self.t0 - 2) * self.Vs // 2
 
     # ---- moving whole fields between the global array and the slabs (set-up, checks) ----------
     def scatter(self, Uglob, xp=np):
@@ -315,19 +320,21 @@ class SlabExchange:
 def emulate_overlapped_pass(slabs, Us, parity: int, run_slices, pending):
     """SlabExchange.parity_pass for all ranks of one process (one GPU or CPU), the ranks' steps
     interleaved in the order the messages allow: every message is a copy and no rank waits on
-    another inside a kernel.  `pending` carries the return messages between passes (start with {};
-    call emulate_finish at the end)."""
+    another inside a kernel.  `run_slices` is one callable for every rank or a list with one per
+    rank (e.g. gpu_step_slices of each slab).  `pending` carries the return messages between
+    passes (start with {}; call emulate_finish at the end)."""
     world = len(slabs)
     p = parity
+    run = run_slices if isinstance(run_slices, (list, tuple)) else [run_slices] * world
     outs = [slabs[r].boundary_out(Us[r], p) for r in range(world)]
     for r in range(world):
-        run_slices(Us[r], slabs[r].local_size, p, 3, slabs[r].T + 1)
+        run[r](Us[r], slabs[r].local_size, p, 3, slabs[r].T + 1)
     emulate_finish(slabs, Us, pending)
     for r in range(world):
-        run_slices(Us[r], slabs[r].local_size, p, slabs[r].T + 1, slabs[r].T + 2)
+        run[r](Us[r], slabs[r].local_size, p, slabs[r].T + 1, slabs[r].T + 2)
     for r in range(world):
         slabs[r].halo_in(Us[r], p, outs[(r - 1) % world])
-        run_slices(Us[r], slabs[r].local_size, p, 2, 3)
+        run[r](Us[r], slabs[r].local_size, p, 2, 3)
     backs = [slabs[r].halo_out(Us[r], p) for r in range(world)]
     pending.update({r: (backs[(r + 1) % world], p) for r in range(world)})
 
@@ -362,6 +369,40 @@ def gpu_or_slices(omega: float = 1.7, gauge: str = "landau", precision: str = "d
         stream = torch.cuda.current_stream().cuda_stream
         _lib.check(_lib.lib().gf_step_slices(g, real, 0, ctypes.c_void_p(U.data_ptr()), s, parity, ctypes.c_float(omega),
                                              0, 0, t_begin, t_end, ctypes.c_void_p(stream)), "gf_step_slices")
+
+    return run
+
+
+def gpu_step_slices(slab: TSlab, algo: str = "or", param: float = 1.7, gauge: str = "landau",
+                    precision: str = "double", seed: int = 0, counter: int = 0):
+    """run_slices for SlabExchange with any update rule: the library's pass over a range of the
+    slab's timeslices (gf_step_slices_at) whose random draws are the whole lattice's
+    (`slab.rng_site_offset`); the pass of parity p draws with counter + p, as the reference's
+    drivers advance the counter per pass."""
+    import ctypes
+
+    from . import _lib
+
+    g = {"landau": _lib.GF_LANDAU, "mag": _lib.GF_MAG, "u1xu1": _lib.GF_U1XU1}.get(gauge)
+    if g is None:
+        raise ValueError("t-slabs are for the 4D gauges (landau, mag, u1xu1)")
+    a = {"or": 0, "micro": 1, "sa": 2, "sr": 3, "random": 4}[algo]
+    real = _lib.GF_FP64 if precision in ("double", "fp64") else _lib.GF_FP32
+    sizes = {}
+
+    def run(U, local_size, parity, t_begin, t_end):
+        if t_end <= t_begin:
+            return
+        s = sizes.get(local_size)
+        if s is None:
+            s = sizes[local_size] = _lib.size_arg(local_size)
+        import torch
+
+        stream = torch.cuda.current_stream().cuda_stream
+        _lib.check(_lib.lib().gf_step_slices_at(g, real, a, ctypes.c_void_p(U.data_ptr()), s, parity,
+                                                ctypes.c_float(param), seed, counter + parity, t_begin, t_end,
+                                                ctypes.c_longlong(slab.rng_site_offset), ctypes.c_void_p(stream)),
+                   "gf_step_slices_at")
 
     return run
 

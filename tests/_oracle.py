@@ -76,13 +76,15 @@ def step(U, size, gauge, algo, parity, param=0.0, seed=0, counter=0, Udw=None, n
                                             ctypes.c_float(param), _u32(seed), _u32(counter), nthreads)
 
 
-def step_slices(U, size, gauge, algo, parity, t_begin, t_end, param=0.0, seed=0, counter=0, nthreads=8):
-    """One parity pass over the sites of timeslices [t_begin, t_end) only, in place."""
+def step_slices(U, size, gauge, algo, parity, t_begin, t_end, param=0.0, seed=0, counter=0, nthreads=8,
+                rng_site_offset=0):
+    """One parity pass over the sites of timeslices [t_begin, t_end) only, in place; site h draws
+    its random numbers as site h + rng_site_offset."""
     half = volume(size) // size[0] // 2
-    getattr(oracle(), "orc_step_range_" + sfx(U))(_ptr(U), None, _ptr(_size(size)), gauge, algo, parity,
-                                                  ctypes.c_float(param), _u32(seed), _u32(counter),
-                                                  ctypes.c_int64(t_begin * half), ctypes.c_int64(t_end * half),
-                                                  nthreads)
+    getattr(oracle(), "orc_step_range_at_" + sfx(U))(_ptr(U), None, _ptr(_size(size)), gauge, algo, parity,
+                                                     ctypes.c_float(param), _u32(seed), _u32(counter),
+                                                     ctypes.c_int64(t_begin * half), ctypes.c_int64(t_end * half),
+                                                     ctypes.c_int64(rng_site_offset), nthreads)
 
 
 def quality(U, size, gauge, stop_max=0, per_site=False, nthreads=8):

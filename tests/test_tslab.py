@@ -13,7 +13,7 @@ import _oracle as O
 from su3_ma_gauge_gpu_b200 import synthetic as S
 from su3_ma_gauge_gpu_b200.tslab import (SlabExchange, TSlab, emulate_finish, emulate_overlapped_pass,
                                         emulate_parity_pass, emulate_refresh_halo, gpu_or_pass, gpu_or_slices,
-                                        parity_pass, quality)
+                                        gpu_step_slices, parity_pass, quality)
 
 SIZE = (8, 4, 6, 4)
 
@@ -108,6 +108,42 @@ def test_emulated_overlapped_slabs_match_single_lattice(world):
     assert np.array_equal(out, _reference(U, 3))
     for s, L, h0 in zip(slabs, Us, halos):  # halo slice 0's parity-0 sites: never updated
         assert np.array_equal(L.reshape(72, -1)[12:, :s.Vs // 2], h0[12:, :s.Vs // 2])
+
+
+@pytest.mark.parametrize("world", [2, 4])
+@pytest.mark.parametrize("gauge,algo,param", [(O.LANDAU, O.SA, 0.8), (O.MAG, O.SA, 0.8), (O.MAG, O.SR, 0.5),
+                                              (O.LANDAU, O.RANDOM, 0.0)])
+def test_emulated_slabs_random_updates_match_single_lattice(world, gauge, algo, param):
+    """Each slab site draws its Philox numbers as its site of the whole lattice
+    (TSlab.rng_site_offset), so the heat bath, stochastic relaxation and random transformations
+    over slabs -- overlapped pass, interior first -- give the single-lattice sweep bit for bit."""
+    U, _ = S.smooth_config(SIZE, 0.3, 37)
+    slabs = [TSlab(SIZE, r, world) for r in range(world)]
+    Us = [s.scatter(U) for s in slabs]
+    R = U.copy()
+    pending = {}
+    for sweep in range(2):
+        for p in (0, 1):
+            ctr = 10 * sweep + p
+            runs = [lambda A, size, parity, t0, t1, s=s, ctr=ctr:
+                    O.step_slices(A, size, gauge, algo, parity, t0, t1, param, 7, ctr, nthreads=2,
+                                  rng_site_offset=s.rng_site_offset) for s in slabs]
+            emulate_overlapped_pass(slabs, Us, p, runs, pending)
+            O.step(R, SIZE, gauge, algo, p, param, 7, ctr, nthreads=2)
+    emulate_finish(slabs, Us, pending)
+    out = np.zeros_like(U)
+    for s, L in zip(slabs, Us):
+        s.gather_into(L, out)
+    assert np.array_equal(out, R)
+
+
+def test_slab_rng_site_offset_maps_local_to_global_sites():
+    """rng_site_offset is the shift between a slab's local and global parity-split indices."""
+    for world in (1, 2, 4):
+        for r in range(world):
+            s = TSlab(SIZE, r, world)
+            assert np.array_equal(s._owned_local % (s.V // 2) + s.rng_site_offset,
+                                  s._owned_global % (int(np.prod(SIZE)) // 2))
 
 
 def _free_port():
@@ -232,3 +268,32 @@ def test_gpu_overlapped_slabs_match_plugin_pass(cuda, world):
     run(B, SIZE, 1, 0, 3)
     run(B, SIZE, 1, 3, SIZE[0])
     assert torch.equal(A, B)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("world", [2, 4])
+@pytest.mark.parametrize("precision", ["double", "float"])
+def test_gpu_slabs_heat_bath_matches_plugin_pass(cuda, world, precision):
+    """The heat bath over slabs with the library's range pass (gf_step_slices_at with each slab's
+    rng_site_offset), ranks emulated on one GPU, against the whole-lattice plugin saStep with the
+    same seed and counters: bit for bit, in FP64 and FP32."""
+    torch = cuda
+    from su3_ma_gauge_gpu_b200 import LandauKernelsSU3
+
+    dt = np.float64 if precision == "double" else np.float32
+    U = S.smooth_config(SIZE, 0.3, 38)[0].astype(dt)
+    dU = torch.from_numpy(U.copy()).cuda()
+    k = LandauKernelsSU3(SIZE, precision)
+    slabs = [TSlab(SIZE, r, world) for r in range(world)]
+    Us = [s.scatter(torch.from_numpy(U.copy()).cuda(), xp=torch) for s in slabs]
+    pending = {}
+    for sweep in range(2):
+        runs = [gpu_step_slices(s, "sa", 0.8, precision=precision, seed=5, counter=10 * sweep) for s in slabs]
+        for p in (0, 1):
+            k.saStep(0, 0, dU, None, p, 0.8, 5, 10 * sweep + p)
+            emulate_overlapped_pass(slabs, Us, p, runs, pending)
+    emulate_finish(slabs, Us, pending)
+    out = torch.zeros_like(dU)
+    for s, L in zip(slabs, Us):
+        s.gather_into(L, out)
+    assert torch.equal(out, dU)
