@@ -81,6 +81,58 @@ __global__ void __launch_bounds__(128) k_parity_pass(F Fup, F Fdw, Geom g, int p
     parity_pass_warp<R, GAUGE, ALGO>(Fup, Fdw, g, warp, parity, p);
 }
 
+// The same pass as a persistent kernel with register prefetch: each warp walks a strided list of
+// 8-site tiles and loads its lane's two links of the next tile into registers before it updates
+// the current one, so a tile's loads are in flight through the arithmetic of the previous one.
+// Odd parities walk the tiles backwards: a driver that calls parity 0 and then parity 1 finds the
+// links the first pass touched last still in L2.  Same site update and stores as k_parity_pass.
+template <typename R, int GAUGE, int ALGO, class F>
+__global__ void __launch_bounds__(128) k_parity_pass_rp(F Fup, F Fdw, Geom g, int parity, AlgoParams p)
+{
+    const int lane = threadIdx.x & 31, mu = lane >> 3;
+    const bool tdown = (GAUGE == COULOMB) && (mu == 0);  // the temporal down link is in slice t-1
+    const int64_t ntiles = g.Vh / 8;
+    const int64_t stride = (int64_t)gridDim.x * 4;
+    int64_t t = (int64_t)blockIdx.x * 4 + (threadIdx.x >> 5);
+    struct Tile {
+        int64_t h, s, sd;
+        R up[12], dn[12];
+    };
+    auto fetch = [&](int64_t k, Tile &r) {
+        const int64_t tile = parity ? ntiles - 1 - k : k;
+        r.h = tile * 8 + (lane & 7);
+        int32_t c[4];
+        site_coords(g, r.h, parity, c);
+        r.s = r.h + (parity ? g.Vh : 0);
+        r.sd = tdown ? r.s : neighbour_down(g, c, mu);
+        Fup.load12(r.s, mu, r.up);
+        if (tdown)
+            Fdw.load12(r.sd, mu, r.dn);
+        else
+            Fup.load12(r.sd, mu, r.dn);
+    };
+    Tile cur;
+    if (t < ntiles) fetch(t, cur);
+    for (; t < ntiles; t += stride) {  // warp-uniform: every lane of a warp runs the same tiles
+        Tile nxt;
+        if (t + stride < ntiles) fetch(t + stride, nxt);
+        Link<R> up, dn;
+        unpack12(up, cur.up);
+        reconstruct(up);
+        unpack12(dn, cur.dn);
+        reconstruct(dn);
+        Rng<R> rng;
+        if (ALGO == ALG_SA || ALGO == ALG_SR || ALGO == ALG_RANDOM) rng.init(ref_rng_tid(cur.h), p.seed, p.counter);
+        site_update<GAUGE, ALGO>(up, dn, mu, p, rng);
+        store_link<R>(Fup, cur.s, mu, up);
+        if (tdown)
+            store_link<R>(Fdw, cur.sd, mu, dn);
+        else
+            store_link<R>(Fup, cur.sd, mu, dn);
+        cur = nxt;
+    }
+}
+
 // One parity pass over the sites of timeslices [t_begin, t_end) only (4D gauges): in the
 // parity-split order those sites are the contiguous run h in [t_begin Vs/2, t_end Vs/2), so the
 // warps cover that run from its 8-aligned start and leave the sites outside it alone.  A t-slab
