@@ -154,7 +154,7 @@ def _free_port():
     return p
 
 
-def _rank(rank, world, port, U, q, overlapped=False):
+def _rank(rank, world, port, U, q, overlapped=False, heat_bath=False):
     import datetime
 
     import torch.distributed as dist
@@ -165,9 +165,13 @@ def _rank(rank, world, port, U, q, overlapped=False):
         slab = TSlab(SIZE, rank, world)
         L = slab.scatter(U)
         ex = SlabExchange(slab, L) if overlapped else None
-        for _ in range(2):
+        for sweep in range(2):
             for p in (0, 1):
-                if overlapped:
+                if heat_bath:  # SA at T = 0.8 with the whole lattice's Philox stream, counter 10 sweep + p
+                    ex.parity_pass(L, p, lambda A, size, parity, t0, t1, c=10 * sweep + p: O.step_slices(
+                        A, size, O.LANDAU, O.SA, parity, t0, t1, 0.8, 7, c, nthreads=2,
+                        rng_site_offset=slab.rng_site_offset))
+                elif overlapped:
                     ex.parity_pass(L, p, _oracle_slices)
                 else:
                     parity_pass(slab, L, p, _oracle_pass)
@@ -207,6 +211,34 @@ def test_gloo_two_ranks_match_single_lattice(overlapped):
     for r in range(2):  # every rank holds the all-reduced sums
         assert res[r][1][0] == pytest.approx(float(g.sum()), rel=1e-13)
         assert res[r][1][1] == pytest.approx(float(a.sum()), rel=1e-11)
+
+
+def test_gloo_two_ranks_heat_bath_matches_single_lattice():
+    """Two gloo ranks with the overlapped exchange run the heat bath, each slab drawing the whole
+    lattice's Philox stream (TSlab.rng_site_offset): the single lattice's SA sweeps bit for bit."""
+    import torch.multiprocessing as mp
+
+    U, _ = S.smooth_config(SIZE, 0.3, 33)
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank, args=(r, 2, port, U, q, True, True)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = [q.get(timeout=180) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    res = {r: o for r, o, _ in got}
+    out = np.zeros_like(U)
+    for r in range(2):
+        sl = TSlab(SIZE, r, 2)
+        out.reshape(72, -1)[:, sl._owned_global] = res[r].reshape(72, -1)[:, sl._owned_global]
+    R = U.copy()
+    for sweep in range(2):
+        for p in (0, 1):
+            O.step(R, SIZE, O.LANDAU, O.SA, p, 0.8, 7, 10 * sweep + p, nthreads=2)
+    assert np.array_equal(out, R)
 
 
 @pytest.mark.gpu
