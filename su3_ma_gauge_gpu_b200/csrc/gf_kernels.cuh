@@ -133,6 +133,88 @@ __global__ void __launch_bounds__(128) k_parity_pass_rp(F Fup, F Fdw, Geom g, in
     }
 }
 
+// FP64 on the reference layout: the same persistent pass with the next tile staged in shared
+// memory by cp.async instead of registers (the register form holds 200 registers in FP64).  In
+// the reference layout every real of a link is its own plane, so a lane copies its two links as
+// 24 eight-byte chunks; chunk k of a lane sits at [stage][k][lane] (conflict-free), and each lane
+// reads back only what it copied, so its own cp.async.wait_group is the only synchronisation.
+constexpr int kRefStageDoubles = 24;  // two links x rows 0, 1 (12 reals each) per lane
+constexpr size_t ref_staged_smem_bytes(int warps) { return (size_t)warps * 2 * kRefStageDoubles * 32 * 8; }
+
+__device__ __forceinline__ void cp_async8_ref(void *smem, const void *gmem)
+{
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+template <int GAUGE, int ALGO>
+__global__ void __launch_bounds__(128) k_parity_pass_ref_staged(RefField<double> Fup, RefField<double> Fdw, Geom g,
+                                                                int parity, AlgoParams p)
+{
+    extern __shared__ double ref_stage[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, mu = lane >> 3;
+    const bool tdown = (GAUGE == COULOMB) && (mu == 0);  // the temporal down link is in slice t-1
+    const int64_t ntiles = g.Vh / 8;
+    const int64_t stride = (int64_t)gridDim.x * 4;
+    double *const wbase = ref_stage + (size_t)w * 2 * kRefStageDoubles * 32;  // this warp's two stages
+    struct Tile {
+        int64_t h, s, sd;
+        bool valid;
+    };
+    auto issue = [&](int64_t k, int st) -> Tile {
+        Tile r{0, 0, 0, k < ntiles};
+        if (r.valid) {
+            const int64_t tile = parity ? ntiles - 1 - k : k;
+            r.h = tile * 8 + (lane & 7);
+            int32_t c[4];
+            site_coords(g, r.h, parity, c);
+            r.s = r.h + (parity ? g.Vh : 0);
+            r.sd = tdown ? r.s : neighbour_down(g, c, mu);
+            double *dst = wbase + (size_t)st * kRefStageDoubles * 32;
+            const double *up = Fup.U + (int64_t)mu * 18 * g.V + r.s;
+            const double *dn = (tdown ? Fdw.U : Fup.U) + (int64_t)mu * 18 * g.V + r.sd;
+#pragma unroll
+            for (int q = 0; q < 12; q++) {
+                cp_async8_ref(dst + q * 32 + lane, up + (int64_t)q * g.V);
+                cp_async8_ref(dst + (12 + q) * 32 + lane, dn + (int64_t)q * g.V);
+            }
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        return r;
+    };
+    int64_t t = (int64_t)blockIdx.x * 4 + w;
+    int cur = 0;
+    Tile tc = issue(t, 0);
+    for (; t < ntiles; t += stride) {  // warp-uniform: every lane of a warp runs the same tiles
+        const Tile tn = issue(t + stride, cur ^ 1);
+        asm volatile("cp.async.wait_group 1;\n" ::: "memory");  // this tile's copies have landed
+        const double *src = wbase + (size_t)cur * kRefStageDoubles * 32;
+        double ru[12], rd[12];
+#pragma unroll
+        for (int q = 0; q < 12; q++) {
+            ru[q] = src[q * 32 + lane];
+            rd[q] = src[(12 + q) * 32 + lane];
+        }
+        Link<double> up, dn;
+        unpack12(up, ru);
+        reconstruct(up);
+        unpack12(dn, rd);
+        reconstruct(dn);
+        Rng<double> rng;
+        if (ALGO == ALG_SA || ALGO == ALG_SR || ALGO == ALG_RANDOM) rng.init(ref_rng_tid(tc.h), p.seed, p.counter);
+        site_update<GAUGE, ALGO>(up, dn, mu, p, rng);
+        store_link<double>(Fup, tc.s, mu, up);
+        if (tdown)
+            store_link<double>(Fdw, tc.sd, mu, dn);
+        else
+            store_link<double>(Fup, tc.sd, mu, dn);
+        __syncwarp();  // every lane is done with this stage before the next iteration refills it
+        tc = tn;
+        cur ^= 1;
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
 // One parity pass over the sites of timeslices [t_begin, t_end) only (4D gauges): in the
 // parity-split order those sites are the contiguous run h in [t_begin Vs/2, t_end Vs/2), so the
 // warps cover that run from its 8-aligned start and leave the sites outside it alone.  A t-slab

@@ -106,6 +106,23 @@ struct RefStep {
             kern<<<blocks, 128, 0, a.stream>>>(fu, fd, a.g, a.parity, a.p);
             return launch_status("parity pass (register prefetch)");
         }
+        if constexpr (ALGO == ALG_OR && sizeof(R) == 8) {
+            // FP64 OR: the persistent pass with the next tile staged by cp.async, one wave of blocks
+            auto kern = k_parity_pass_ref_staged<GAUGE, ALGO>;
+            const size_t smem = ref_staged_smem_bytes(4);  // 48 KB: no opt-in needed
+            static int per_sm = 0, sms = 0;
+            if (per_sm <= 0) {
+                int dev = 0, o = 0;
+                cudaGetDevice(&dev);
+                cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, kern, 128, smem) != cudaSuccess || o < 1) o = 1;
+                per_sm = o;
+            }
+            const int64_t need = (ntiles + 3) / 4;
+            const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>(need, (int64_t)sms * per_sm));
+            kern<<<blocks, 128, smem, a.stream>>>(fu, fd, a.g, a.parity, a.p);
+            return launch_status("parity pass (cp.async pipelined)");
+        }
         const int64_t threads = a.g.Vh * 4;
         const unsigned blocks = (unsigned)((threads + 127) / 128);
         k_parity_pass<R, GAUGE, ALGO, RefField<R>><<<blocks, 128, 0, a.stream>>>(fu, fd, a.g, a.parity, a.p);
