@@ -1401,16 +1401,16 @@ int gf_autotune(gf_ctx *c, int *choice_fp32, int *choice_fp64)
         float best = 1e30f;
         int besti = 0;
         const long long keep = c->launches;
-        // two rounds over all candidates, each candidate's time the faster of its two: candidates a
+        // three rounds over all candidates, each candidate's time the fastest of its three: shapes a
         // few per cent apart (FP64 at 32^4) are not ranked by one sample taken while the clock ramps
         std::vector<float> tmin(ncand, 1e30f);
-        for (int round = 0; round < 2 && !st; round++) {
+        for (int round = 0; round < 3 && !st; round++) {
             for (int k = 0; k < ncand && !st; k++) {
                 gf_ctx::PassShape sh[2] = {c->shape[0], c->shape[1]};
                 sh[prec] = cands[k];
-                for (int w = 0; w < 2 - round && !st; w++) st = launch_sweep_on(c, e, sh, ALG_OR, want, 1.7f, 0, 0, 0);
+                for (int w = 0; w < (round ? 1 : 2) && !st; w++) st = launch_sweep_on(c, e, sh, ALG_OR, want, 1.7f, 0, 0, 0);
                 cudaEventRecord(e0, c->stream);
-                for (int w = 0; w < 3 && !st; w++) st = launch_sweep_on(c, e, sh, ALG_OR, want, 1.7f, 0, 0, 0);
+                for (int w = 0; w < 4 && !st; w++) st = launch_sweep_on(c, e, sh, ALG_OR, want, 1.7f, 0, 0, 0);
                 cudaEventRecord(e1, c->stream);
                 if (!st) st = cuda_status(cudaEventSynchronize(e1), "autotune sync");
                 float ms = 0;
